@@ -1,0 +1,329 @@
+/*
+ * swift_b200.h -- C ABI of the B200-native Swift SpMM library (libswiftb200.so).
+ *
+ * Swift computes C = A * B for a CSR sparse A (M x K) and a dense B (K x N).  The library
+ * builds the Swift column-sorted tiled format ON THE GPU (column sort by nonzero count,
+ * 32-nonzero regular tiles, irregular "reside" remainder, load-balance blocks), keeps it
+ * resident in HBM as a plan, and runs hand-written sm_100a kernels over it.
+ *
+ * All entry points are plain C: pointers, sizes and enums only.  Every call returns a
+ * swift_status; nothing prints and nothing exits.  Device work is stream-ordered on the
+ * caller's stream (NULL = the legacy default stream).  Plans are immutable after creation
+ * and may be used concurrently from several streams.
+ *
+ * Reference interface each entry point replaces (paths inside the reference project):
+ *   swift_plan_create           -- csr_to_csc + col_sort/ColSort + formattransation/
+ *                                  formatTransform + block_catgory + balance, as sequenced
+ *                                  by src/main.cu:207-385 (src/gpu_csr2csc.h:51,
+ *                                  src/coo2csc.h:82,137, src/ColSort_cuda.h:48,
+ *                                  src/formatTransform_cuda.h:198, src/block_catgory.h:1,
+ *                                  src/balance.h:1)
+ *   swift_plan_export_*         -- the slide_matrix those functions fill (src/format.h:6-39)
+ *   swift_spmm                  -- Swift_GPU / Swift_GPU_3 / Swift_GPU_4 / Swift_gpu1 /
+ *                                  Swift_gpu2 kernels (src/Swift.h:15-181,
+ *                                  src/Swift_3.h:6-213, src/Swift_4.h:6-302,
+ *                                  src/Swift_gpu_col_major.h:6-168,
+ *                                  src/Swift_gpu_row_major.h:29-133)
+ *   swift_ref_*                 -- the same functions with the reference's host-buffer
+ *                                  calling convention (see swift_compat.h for the C++ shims
+ *                                  that carry the reference's exact signatures)
+ *   swift_spmm_transposed, swift_sddmm, swift_fused_forward_backward, swift_batch_*
+ *                               -- no counterpart in the reference (backward pass and
+ *                                  batched execution added by this library)
+ */
+#ifndef SWIFT_B200_H
+#define SWIFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is exported from the shared library (built with hidden default
+ * visibility). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define SWIFT_B200_VERSION "0.1.0"
+
+/* Same object as cudaStream_t; NULL selects the legacy default stream. */
+typedef struct CUstream_st *swift_stream_t;
+
+typedef enum swift_status {
+  SWIFT_OK = 0,
+  SWIFT_ERR_INVALID_ARG = 1, /* null pointer, negative size, unknown enum value           */
+  SWIFT_ERR_BAD_CSR = 2,     /* rowptr not monotone / not 0..nnz, column index out of range */
+  SWIFT_ERR_BAD_PERM = 3,    /* injected column order is not a count-sorting permutation  */
+  SWIFT_ERR_UNSUPPORTED = 4, /* dtype / layout / engine combination not provided          */
+  SWIFT_ERR_CUDA = 5,        /* a CUDA runtime call or kernel launch failed               */
+  SWIFT_ERR_ALLOC = 6,       /* device or host allocation failed                          */
+  SWIFT_ERR_OVERFLOW = 7,    /* a size exceeds the int32 index range of the format        */
+  SWIFT_ERR_TIMEOUT = 8,     /* a bounded device-side wait ran out                        */
+  SWIFT_ERR_NO_DEVICE = 9,   /* no CUDA device, or not an sm_100 device                   */
+  SWIFT_ERR_VERIFY = 10      /* compat entry points: result differs from the golden C     */
+} swift_status;
+
+typedef enum swift_dtype { SWIFT_F32 = 0, SWIFT_F64 = 1, SWIFT_BF16 = 2, SWIFT_F16 = 3 } swift_dtype;
+typedef enum swift_layout { SWIFT_ROW_MAJOR = 0, SWIFT_COL_MAJOR = 1 } swift_layout;
+typedef enum swift_memspace { SWIFT_HOST = 0, SWIFT_DEVICE = 1 } swift_memspace;
+
+/* Execution engines over the same plan.
+ *   TILED   -- the Swift kernels proper: one warp per run of regular tiles that share their
+ *              32 sorted columns, runs of equal rows reduced in registers before a vector
+ *              atomic into C, plus the load-balanced reside blocks.  Any layout of B and C.
+ *   ROWWISE -- row-ordered execution for C much larger than L2: each C row is accumulated
+ *              in registers and written once; rows longer than the split threshold are cut
+ *              into pieces combined deterministically.  Row-major B and C.
+ *   AUTO    -- the autotuned choice for (N, dtype), ROWWISE when no tuning was run and the
+ *              layouts allow it. */
+typedef enum swift_engine { SWIFT_ENGINE_AUTO = 0, SWIFT_ENGINE_TILED = 1, SWIFT_ENGINE_ROWWISE = 2 } swift_engine;
+
+typedef struct swift_csr {
+  int rows;              /* M */
+  int cols;              /* K */
+  int nnz;
+  const int *rowptr;     /* M+1, rowptr[0] = 0, non-decreasing, rowptr[M] = nnz */
+  const int *colidx;     /* nnz, each in [0, K) */
+  const void *val;       /* nnz values of type val_type */
+  swift_dtype val_type;  /* SWIFT_F32 or SWIFT_F64 */
+  swift_memspace mem;    /* where rowptr/colidx/val live */
+} swift_csr;
+
+typedef struct swift_plan_opts {
+  /* Column order to use instead of the stable count order (ascending count, ties by
+   * ascending column index -- the order of the reference's thrust::sort_by_key,
+   * src/ColSort_cuda.h:108).  Must sort the column counts ascending.  NULL = stable. */
+  const int *col_perm;
+  swift_memspace col_perm_mem;
+  /* Rowwise engine: rows with more nonzeros than this are cut into pieces of this size
+   * (0 = default 128). */
+  int long_row_split;
+  /* Also build the transposed (A^T) row layout used by swift_spmm_transposed and the
+   * backward kernels (0 = build lazily on first use). */
+  int build_transpose;
+} swift_plan_opts;
+
+typedef struct swift_plan swift_plan;
+
+typedef struct swift_plan_stats {
+  int rows, cols, nnz;
+  int nsteps;            /* distinct nonzero counts among the sorted columns */
+  int tilenum, regular_nnz;
+  int reside_col, reside_nnz, numblk;
+  int fmt_count[3];      /* regular tiles of format 0 / 1 / 2 (src/block_catgory.h) */
+  int empty_cols, max_col_nnz, max_row_nnz;
+  int long_rows, long_pieces, long_row_split;
+  double build_ms;       /* device time of the format build (CUDA events) */
+  size_t device_bytes;   /* HBM held by the plan */
+} swift_plan_stats;
+
+/* Host copy of the reference's slide_matrix, field for field (src/format.h:6-39).  The
+ * FP32 flavour matches test/k-32/FP32/format.h; a reference slide_matrix* may be passed
+ * where these are expected.  Arrays are malloc'd; free with swift_slide_free_* or the
+ * reference's Tile_destroy. */
+#define SWIFT_SLIDE_FIELDS(VAL_T)                                                             \
+  VAL_T *sortval;                                                                             \
+  int *sortrowidx;                                                                            \
+  int *tile_ptr;                                                                              \
+  int *tile_len;                                                                              \
+  int *tile_colidx;                                                                           \
+  int *tile_tall;                                                                             \
+  int *tile_format;                                                                           \
+  int *countrow;                                                                              \
+  int *segmentoffset;                                                                         \
+  int *segptr;                                                                                \
+  int *seginfo;                                                                               \
+  int *seglength;                                                                             \
+  int *sortrowindex;                                                                          \
+  int *val_position;                                                                          \
+  int *val_offset;                                                                            \
+  int tilenum;                                                                                \
+  int segsum;                                                                                 \
+  int regular_nnz;                                                                            \
+  int reside_col;                                                                             \
+  int reside_nnz;                                                                             \
+  int *reside_cscptr;                                                                         \
+  int *reside_cscrowidx;                                                                      \
+  VAL_T *reside_val;                                                                          \
+  int numblk;                                                                                 \
+  unsigned int *colorblk;                                                                     \
+  int *blkstart;                                                                              \
+  int *blkstop;                                                                               \
+  int *blkptr;
+
+typedef struct swift_slide_matrix_f32 { SWIFT_SLIDE_FIELDS(float) } swift_slide_matrix_f32;
+typedef struct swift_slide_matrix_f64 { SWIFT_SLIDE_FIELDS(double) } swift_slide_matrix_f64;
+
+/* ------------------------------------------------------------------ basics */
+const char *swift_status_string(swift_status s);
+const char *swift_version(void);
+/* Text of the last CUDA or validation failure seen by this thread ("" if none). */
+const char *swift_last_error(void);
+/* Checks that a CUDA device of compute capability 10.x is current. */
+swift_status swift_device_check(int *sm_count, int *cc_major, int *cc_minor);
+
+/* ------------------------------------------------------------------ plans */
+/* Builds the Swift format of A on the current device.  A may live on the host or the
+ * device.  Synchronises `stream` once (sizes of the format are read back). */
+swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
+                               swift_stream_t stream, swift_plan **out);
+swift_status swift_plan_destroy(swift_plan *plan);
+swift_status swift_plan_get_stats(const swift_plan *plan, swift_plan_stats *out);
+
+/* Host copies of every reference array.  with_row_sort != 0 also runs the per-8-tile row
+ * sort (src/back_process.h:23-229) and fills val_position / val_offset; the reference
+ * overwrites sortrowidx with the sorted keys at that point, and so does this export.
+ * blockratio (may be NULL) receives the FP32 flavour's statistic of that step. */
+swift_status swift_plan_export_f32(const swift_plan *plan, swift_slide_matrix_f32 *out,
+                                   int with_row_sort, float *blockratio);
+swift_status swift_plan_export_f64(const swift_plan *plan, swift_slide_matrix_f64 *out,
+                                   int with_row_sort, float *blockratio);
+void swift_slide_free_f32(swift_slide_matrix_f32 *m);
+void swift_slide_free_f64(swift_slide_matrix_f64 *m);
+
+/* Host copies of the column sort (src/coo2csc.h:82-134 outputs): perm[K] (sorted position ->
+ * column), sortnnz[K], and the sorted CSC (nnz row indices / values of the plan's type).
+ * Any pointer may be NULL. */
+swift_status swift_plan_export_sorted(const swift_plan *plan, int *perm, int *sortnnz,
+                                      int *sortrowidx_tmp, void *sortval_tmp);
+
+/* ------------------------------------------------------------------ products */
+/* C = A * B.  B is K x N, C is M x N, both of `dtype` (F32 or F64 matching the plan's
+ * values, or BF16 / F16 with an F32 plan: B and C in 16 bits, products accumulated in F32).
+ * ld* are leading dimensions in elements (row-major: row stride; col-major: column
+ * stride).  b_presorted != 0 means B's rows are already in the plan's sorted column order
+ * (the reference's sort_dense_mtx); otherwise rows are in A's original column order.
+ * C is overwritten.  Stream-ordered; no synchronisation. */
+swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swift_dtype dtype,
+                        const void *B, int64_t ldb, swift_layout b_layout, int b_presorted,
+                        void *C, int64_t ldc, swift_layout c_layout, swift_stream_t stream);
+
+/* X = A^T * Y (row-major, K x N and M x N): the backward product dX = A^T dY. */
+swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dtype,
+                                   const void *Y, int64_t ldy, void *X, int64_t ldx,
+                                   swift_stream_t stream);
+
+/* out[e] = sum_n U[row_e, n] * V[col_e, n] for every nonzero e of A in CSR order
+ * (U is M x N, V is K x N, row-major): the backward dA_vals = SDDMM(dY, X).  out has the
+ * plan's value type (F32 plans accumulate F32, also for BF16/F16 inputs). */
+swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const void *U,
+                         int64_t ldu, const void *V, int64_t ldv, void *out,
+                         swift_stream_t stream);
+
+/* One pass over A in row order for Y = A X and dA_vals = SDDMM(dY, X) (X read once per
+ * nonzero for both), then dX = A^T dY over the transposed layout.  Any output pointer may be
+ * NULL to skip that product.  Row-major, F32 or F64. */
+swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_dtype dtype,
+                                          const void *X, int64_t ldx, const void *dY,
+                                          int64_t lddy, void *Y, int64_t ldy, void *dX,
+                                          int64_t lddx, void *dA, swift_stream_t stream);
+
+/* Deterministic FP64 product C = A * B (one warp per row, nonzeros summed in CSR order),
+ * the GPU error reference; A's values are widened if the plan is F32.  Row-major. */
+swift_status swift_spmm_f64_reference(const swift_plan *plan, int N, const double *B,
+                                      int64_t ldb, double *C, int64_t ldc,
+                                      swift_stream_t stream);
+
+/* ------------------------------------------------------------------ tuning */
+/* Times the engines and their parameters on this plan for (N, dtype) with CUDA events and
+ * stores the fastest as the plan's AUTO choice.  B and C are caller buffers of the right
+ * shape (row-major); their contents are overwritten.  best_ms may be NULL. */
+swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, const void *B,
+                                 void *C, swift_stream_t stream, double *best_ms,
+                                 swift_engine *best_engine);
+
+/* ------------------------------------------------------------------ batches */
+/* Many independent products C_i = A_i * B_i (row-major, F32) in one persistent launch. */
+typedef struct swift_batch swift_batch;
+swift_status swift_batch_create(swift_plan *const *plans, int count, swift_stream_t stream,
+                                swift_batch **out);
+swift_status swift_batch_destroy(swift_batch *batch);
+/* Ns[i], B[i], ldb[i], C[i], ldc[i] per matrix (device pointers, row-major).  Capturable in
+ * a CUDA graph once set: swift_batch_set_operands uploads the operand table, then
+ * swift_batch_run only launches. */
+swift_status swift_batch_set_operands(swift_batch *batch, const int *Ns, const void *const *B,
+                                      const int64_t *ldb, void *const *C, const int64_t *ldc,
+                                      swift_stream_t stream);
+swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream);
+/* Captures swift_batch_run into a CUDA graph and replays it (graph kept by the batch). */
+swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream);
+
+/* ------------------------------------------------------------------ reference calling convention */
+/* The reference's preprocessing and kernels with its host-buffer convention: inputs and
+ * outputs are host arrays, device buffers are allocated and freed inside, and *ms receives
+ * the device time of the work (CUDA events) where the reference reports a time.  Column
+ * sorts use the stable count order.  swift_compat.h wraps these in the reference's C++
+ * signatures. */
+swift_status swift_ref_csr_to_csc_f32(float *ms, int m, int n, int nnz, const float *csr_val,
+                                      const int *csr_row_ptr, const int *csr_col_ind,
+                                      float *csc_val, int *csc_row_ind, int *csc_col_ptr,
+                                      int *nnzpercol);
+swift_status swift_ref_csr_to_csc_f64(float *ms, int m, int n, int nnz, const double *csr_val,
+                                      const int *csr_row_ptr, const int *csr_col_ind,
+                                      double *csc_val, int *csc_row_ind, int *csc_col_ptr,
+                                      int *nnzpercol);
+/* src/coo2csc.h:82-134 / src/ColSort_cuda.h:48-143 */
+swift_status swift_ref_col_sort_f32(float *ms, int colA, int nnz, int width, const int *nnzpercol,
+                                    const int *csccolptr, const int *cscrowidx,
+                                    const float *cscval, int *sortrowidx_tmp,
+                                    float *sortval_tmp, int *sortnnz_tmp, const float *dense,
+                                    float *sort_dense);
+swift_status swift_ref_col_sort_f64(float *ms, int colA, int nnz, int width, const int *nnzpercol,
+                                    const int *csccolptr, const int *cscrowidx,
+                                    const double *cscval, int *sortrowidx_tmp,
+                                    double *sortval_tmp, int *sortnnz_tmp, const double *dense,
+                                    double *sort_dense);
+/* src/coo2csc.h:137-435 (regular + reside).  reside_ratio may be NULL. */
+swift_status swift_ref_formattransation_f32(float *ms, swift_slide_matrix_f32 *m,
+                                            const int *sortrowidx_tmp, const float *sortval_tmp,
+                                            const int *sortnnz_tmp, int nnz, int rowA, int colA,
+                                            double *reside_ratio);
+swift_status swift_ref_formattransation_f64(float *ms, swift_slide_matrix_f64 *m,
+                                            const int *sortrowidx_tmp, const double *sortval_tmp,
+                                            const int *sortnnz_tmp, int nnz, int rowA, int colA,
+                                            double *reside_ratio);
+/* src/formatTransform_cuda.h:198-435 (regular part only; h_count = number of steps). */
+swift_status swift_ref_formatTransform_f32(float *ms, swift_slide_matrix_f32 *m,
+                                           const int *sortrowidx_tmp, const float *sortval_tmp,
+                                           const int *sortnnz_tmp, int nnz, int rowA, int colA,
+                                           int *h_count);
+swift_status swift_ref_formatTransform_f64(float *ms, swift_slide_matrix_f64 *m,
+                                           const int *sortrowidx_tmp, const double *sortval_tmp,
+                                           const int *sortnnz_tmp, int nnz, int rowA, int colA,
+                                           int *h_count);
+/* src/block_catgory.h:1-160.  shuffle_ratio may be NULL. */
+swift_status swift_ref_block_catgory_f32(swift_slide_matrix_f32 *m, double *shuffle_ratio);
+swift_status swift_ref_block_catgory_f64(swift_slide_matrix_f64 *m, double *shuffle_ratio);
+/* src/balance.h:1-69 */
+swift_status swift_ref_balance_f32(swift_slide_matrix_f32 *m, int m_rows, int n_reside,
+                                   int reside_nnz, const int *cscptr, const int *cscrowidx);
+swift_status swift_ref_balance_f64(swift_slide_matrix_f64 *m, int m_rows, int n_reside,
+                                   int reside_nnz, const int *cscptr, const int *cscrowidx);
+/* src/back_process.h:23-229.  blockratio may be NULL. */
+swift_status swift_ref_row_idx_sort_f32(swift_slide_matrix_f32 *m, int rowA, int colA,
+                                        int width, float *blockratio);
+swift_status swift_ref_row_idx_sort_f64(swift_slide_matrix_f64 *m, int rowA, int colA,
+                                        int width, float *blockratio);
+/* Swift_GPU (variant 0), Swift_gpu1 (1), Swift_gpu2 (2), Swift_GPU_3 (3), Swift_GPU_4 (4):
+ * C = A * B from a host slide_matrix.  B is the column-sorted dense operand, column-major
+ * (K x N, leading dimension K) for every variant except 2, which takes it row-major
+ * (K x N, leading dimension N); C is returned in the same layout (M x N).  The reference
+ * wrappers' timing window (kernels only) is reported in *ms. */
+swift_status swift_ref_spmm_f32(int variant, const swift_slide_matrix_f32 *m, int rowA,
+                                int colA, int width, int nnz, const float *h_B_sorted,
+                                float *h_C, float *ms);
+swift_status swift_ref_spmm_f64(int variant, const swift_slide_matrix_f64 *m, int rowA,
+                                int colA, int width, int nnz, const double *h_B_sorted,
+                                double *h_C, float *ms);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWIFT_B200_H */

@@ -1,0 +1,380 @@
+// capi.cu -- extern "C" entry points of libswiftb200.so (declared in include/swift_b200.h).
+#include <chrono>
+#include <cstdlib>
+
+#include "common.cuh"
+
+namespace swift {
+
+template <class VAL_T, class SLIDE>
+swift_status export_slide(const Plan &p, SLIDE *out, int with_row_sort, float *blockratio,
+                          cudaStream_t st);
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const char *where, const char *what) {
+  g_last_error = std::string(where) + ": " + what;
+}
+
+size_t plan_device_bytes(const Plan &p) {
+  const DevBuf *bufs[] = {&p.rowptr, &p.colidx, &p.val, &p.cnt, &p.perm, &p.invperm, &p.sortnnz,
+                          &p.sptr, &p.srow, &p.sval, &p.spos, &p.step_col, &p.step_base,
+                          &p.step_tall, &p.step_tile_off, &p.item_tile, &p.tile_colidx,
+                          &p.tile_depth, &p.tile_tall, &p.tile_format, &p.sortrowidx, &p.sortval,
+                          &p.reside_ptr, &p.reside_row, &p.reside_val, &p.colorblk, &p.blkstart,
+                          &p.blkstop, &p.blkptr};
+  size_t s = 0;
+  for (const DevBuf *b : bufs) s += b->bytes;
+  for (const RowLayout *L : {&p.fwd, &p.bwd}) {
+    const DevBuf *lb[] = {&L->piece_row, &L->piece_idx, &L->long_first, &L->long_count,
+                          &L->long_of_row, &L->counters, &L->scratch};
+    for (const DevBuf *b : lb) s += b->bytes;
+  }
+  return s;
+}
+
+static swift_status check_device(int *sm_count) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { set_last_error("cudaGetDevice", cudaGetErrorString(e)); return SWIFT_ERR_NO_DEVICE; }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) { set_last_error("cudaGetDeviceProperties", cudaGetErrorString(e)); return SWIFT_ERR_NO_DEVICE; }
+  if (prop.major != 10) {
+    set_last_error("device", "libswiftb200 is built for sm_100a (compute capability 10.x) only");
+    return SWIFT_ERR_NO_DEVICE;
+  }
+  if (sm_count) *sm_count = prop.multiProcessorCount;
+  return SWIFT_OK;
+}
+
+static size_t dtype_size(swift_dtype d) {
+  switch (d) {
+    case SWIFT_F32: return 4;
+    case SWIFT_F64: return 8;
+    case SWIFT_BF16:
+    case SWIFT_F16: return 2;
+  }
+  return 0;
+}
+
+swift_status ensure_bwd(Plan &p, cudaStream_t st) {
+  std::lock_guard<std::mutex> g(p.mu);
+  if (p.bwd.built) return SWIFT_OK;
+  return build_row_layout(p, p.bwd, true, st);
+}
+
+}  // namespace swift
+
+using namespace swift;
+
+struct swift_plan {
+  Plan p;
+};
+
+extern "C" {
+
+const char *swift_status_string(swift_status s) {
+  switch (s) {
+    case SWIFT_OK: return "ok";
+    case SWIFT_ERR_INVALID_ARG: return "invalid argument";
+    case SWIFT_ERR_BAD_CSR: return "malformed CSR input";
+    case SWIFT_ERR_BAD_PERM: return "column permutation does not sort the column counts";
+    case SWIFT_ERR_UNSUPPORTED: return "unsupported dtype / layout / engine combination";
+    case SWIFT_ERR_CUDA: return "CUDA error";
+    case SWIFT_ERR_ALLOC: return "allocation failed";
+    case SWIFT_ERR_OVERFLOW: return "size exceeds the int32 index range";
+    case SWIFT_ERR_TIMEOUT: return "bounded device wait timed out";
+    case SWIFT_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case SWIFT_ERR_VERIFY: return "result differs from the golden product";
+  }
+  return "unknown status";
+}
+
+const char *swift_version(void) { return SWIFT_B200_VERSION; }
+
+const char *swift_last_error(void) { return g_last_error.c_str(); }
+
+swift_status swift_device_check(int *sm_count, int *cc_major, int *cc_minor) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { set_last_error("cudaGetDevice", cudaGetErrorString(e)); return SWIFT_ERR_NO_DEVICE; }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) return SWIFT_ERR_NO_DEVICE;
+  if (sm_count) *sm_count = prop.multiProcessorCount;
+  if (cc_major) *cc_major = prop.major;
+  if (cc_minor) *cc_minor = prop.minor;
+  return prop.major == 10 ? SWIFT_OK : SWIFT_ERR_NO_DEVICE;
+}
+
+swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
+                               swift_stream_t stream, swift_plan **out) {
+  if (!A || !out) return SWIFT_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (A->rows < 0 || A->cols < 0 || A->nnz < 0 || !A->rowptr) return SWIFT_ERR_INVALID_ARG;
+  if (A->nnz > 0 && (!A->colidx || !A->val)) return SWIFT_ERR_INVALID_ARG;
+  if (A->val_type != SWIFT_F32 && A->val_type != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+  if (A->mem != SWIFT_HOST && A->mem != SWIFT_DEVICE) return SWIFT_ERR_INVALID_ARG;
+  if (A->mem == SWIFT_HOST) {
+    // cheap host-side validation before anything is uploaded
+    if (A->rowptr[0] != 0 || A->rowptr[A->rows] != A->nnz) return SWIFT_ERR_BAD_CSR;
+    for (int i = 0; i < A->rows; ++i)
+      if (A->rowptr[i] > A->rowptr[i + 1]) return SWIFT_ERR_BAD_CSR;
+    for (int i = 0; i < A->nnz; ++i)
+      if (A->colidx[i] < 0 || A->colidx[i] >= A->cols) return SWIFT_ERR_BAD_CSR;
+  }
+  int sms = 0;
+  SW_TRY(check_device(&sms));
+  cudaStream_t st = S(stream);
+  swift_plan *h = new (std::nothrow) swift_plan;
+  if (!h) return SWIFT_ERR_ALLOC;
+  Plan &p = h->p;
+  p.M = A->rows; p.K = A->cols; p.nnz = A->nnz;
+  cudaGetDevice(&p.device);
+  p.sm_count = sms;
+  p.val_type = A->val_type;
+  p.vsz = dtype_size(A->val_type);
+  p.long_row_split = (opts && opts->long_row_split > 0) ? opts->long_row_split : 128;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  swift_status rc = build_from_csr(p, *A, opts, st);
+  if (rc == SWIFT_OK) rc = build_row_layout(p, p.fwd, false, st);
+  if (rc == SWIFT_OK && opts && opts->build_transpose) rc = ensure_bwd(p, st);
+  cudaEventRecord(e1, st);
+  if (rc == SWIFT_OK) {
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) { set_last_error("plan build", cudaGetErrorString(e)); rc = SWIFT_ERR_CUDA; }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    p.build_ms = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != SWIFT_OK) {
+    cudaStreamSynchronize(st);
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_destroy(swift_plan *plan) {
+  if (!plan) return SWIFT_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  delete plan;
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_get_stats(const swift_plan *plan, swift_plan_stats *o) {
+  if (!plan || !o) return SWIFT_ERR_INVALID_ARG;
+  const Plan &p = plan->p;
+  memset(o, 0, sizeof(*o));
+  o->rows = p.M; o->cols = p.K; o->nnz = p.nnz;
+  o->nsteps = p.nsteps; o->tilenum = p.tilenum; o->regular_nnz = p.tilenum * kTile;
+  o->reside_col = p.reside_col; o->reside_nnz = p.reside_nnz; o->numblk = p.numblk;
+  for (int i = 0; i < 3; ++i) o->fmt_count[i] = p.fmt_count[i];
+  o->max_col_nnz = p.max_col; o->max_row_nnz = p.max_row; o->empty_cols = p.empty_cols;
+  o->long_rows = p.fwd.long_rows; o->long_pieces = p.fwd.pieces; o->long_row_split = p.fwd.split;
+  o->build_ms = p.build_ms;
+  o->device_bytes = plan_device_bytes(p);
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_export_f32(const swift_plan *plan, swift_slide_matrix_f32 *out,
+                                   int with_row_sort, float *blockratio) {
+  if (!plan || !out) return SWIFT_ERR_INVALID_ARG;
+  if (plan->p.val_type != SWIFT_F32) return SWIFT_ERR_UNSUPPORTED;
+  return export_slide<float>(plan->p, out, with_row_sort, blockratio, nullptr);
+}
+
+swift_status swift_plan_export_f64(const swift_plan *plan, swift_slide_matrix_f64 *out,
+                                   int with_row_sort, float *blockratio) {
+  if (!plan || !out) return SWIFT_ERR_INVALID_ARG;
+  if (plan->p.val_type != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+  return export_slide<double>(plan->p, out, with_row_sort, blockratio, nullptr);
+}
+
+#define SWIFT_SLIDE_FREE(m)                                                                   \
+  do {                                                                                        \
+    void *ps[] = {m->sortval, m->sortrowidx, m->tile_ptr, m->tile_len, m->tile_colidx,        \
+                  m->tile_tall, m->tile_format, m->countrow, m->segmentoffset, m->segptr,     \
+                  m->seginfo, m->seglength, m->sortrowindex, m->val_position, m->val_offset,  \
+                  m->reside_cscptr, m->reside_cscrowidx, m->reside_val, m->colorblk,          \
+                  m->blkstart, m->blkstop, m->blkptr};                                        \
+    for (void *q : ps) free(q);                                                               \
+    memset(m, 0, sizeof(*m));                                                                 \
+  } while (0)
+
+void swift_slide_free_f32(swift_slide_matrix_f32 *m) { if (m) SWIFT_SLIDE_FREE(m); }
+void swift_slide_free_f64(swift_slide_matrix_f64 *m) { if (m) SWIFT_SLIDE_FREE(m); }
+
+swift_status swift_plan_export_sorted(const swift_plan *plan, int *perm, int *sortnnz,
+                                      int *sortrowidx_tmp, void *sortval_tmp) {
+  if (!plan) return SWIFT_ERR_INVALID_ARG;
+  const Plan &p = plan->p;
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  if (perm) SW_CHECK_CUDA(cudaMemcpy(perm, p.perm.p, sizeof(int) * (size_t)p.K, cudaMemcpyDeviceToHost));
+  if (sortnnz) SW_CHECK_CUDA(cudaMemcpy(sortnnz, p.sortnnz.p, sizeof(int) * (size_t)p.K, cudaMemcpyDeviceToHost));
+  if (sortrowidx_tmp) SW_CHECK_CUDA(cudaMemcpy(sortrowidx_tmp, p.srow.p, sizeof(int) * (size_t)p.nnz, cudaMemcpyDeviceToHost));
+  if (sortval_tmp) SW_CHECK_CUDA(cudaMemcpy(sortval_tmp, p.sval.p, p.vsz * (size_t)p.nnz, cudaMemcpyDeviceToHost));
+  return SWIFT_OK;
+}
+
+static swift_status check_dense(const swift_plan *plan, int N, swift_dtype dt, const void *B,
+                                int64_t ldb, swift_layout bl, int brows, const void *C,
+                                int64_t ldc, swift_layout cl, int crows) {
+  if (!plan || N < 0) return SWIFT_ERR_INVALID_ARG;
+  if (dtype_size(dt) == 0) return SWIFT_ERR_INVALID_ARG;
+  if ((bl != SWIFT_ROW_MAJOR && bl != SWIFT_COL_MAJOR) || (cl != SWIFT_ROW_MAJOR && cl != SWIFT_COL_MAJOR))
+    return SWIFT_ERR_INVALID_ARG;
+  if (N == 0) return SWIFT_OK;
+  if ((brows > 0 && !B) || (crows > 0 && !C)) return SWIFT_ERR_INVALID_ARG;
+  if (ldb < (bl == SWIFT_ROW_MAJOR ? N : std::max(brows, 1))) return SWIFT_ERR_INVALID_ARG;
+  if (ldc < (cl == SWIFT_ROW_MAJOR ? N : std::max(crows, 1))) return SWIFT_ERR_INVALID_ARG;
+  const Plan &p = plan->p;
+  if (p.val_type == SWIFT_F64 && dt != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+  if (p.val_type == SWIFT_F32 && dt == SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+  return SWIFT_OK;
+}
+
+swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swift_dtype dtype,
+                        const void *B, int64_t ldb, swift_layout b_layout, int b_presorted,
+                        void *C, int64_t ldc, swift_layout c_layout, swift_stream_t stream) {
+  SW_TRY(check_dense(plan, N, dtype, B, ldb, b_layout, plan ? plan->p.K : 0, C, ldc, c_layout,
+                     plan ? plan->p.M : 0));
+  Plan &p = const_cast<Plan &>(plan->p);
+  DenseArgs d;
+  d.N = N; d.dtype = dtype; d.B = B; d.ldb = ldb; d.b_layout = b_layout; d.b_presorted = b_presorted != 0;
+  d.C = C; d.ldc = ldc; d.c_layout = c_layout;
+  cudaStream_t st = S(stream);
+  const bool row_ok = p.has_csr && b_layout == SWIFT_ROW_MAJOR && c_layout == SWIFT_ROW_MAJOR && !b_presorted;
+  if (engine == SWIFT_ENGINE_AUTO) {
+    engine = row_ok ? SWIFT_ENGINE_ROWWISE : SWIFT_ENGINE_TILED;
+    std::lock_guard<std::mutex> g(p.mu);
+    auto it = p.tuned.find({N, (int)dtype});
+    if (it != p.tuned.end() && (it->second == SWIFT_ENGINE_TILED || row_ok)) engine = it->second;
+  }
+  if (engine == SWIFT_ENGINE_ROWWISE) {
+    if (!row_ok) return SWIFT_ERR_UNSUPPORTED;
+    if (p.M == 0) return SWIFT_OK;
+    return run_rowwise(p, p.fwd, d, st);
+  }
+  if (engine == SWIFT_ENGINE_TILED) return run_tiled(p, d, 0, st);
+  return SWIFT_ERR_INVALID_ARG;
+}
+
+swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dtype,
+                                   const void *Y, int64_t ldy, void *X, int64_t ldx,
+                                   swift_stream_t stream) {
+  SW_TRY(check_dense(plan, N, dtype, Y, ldy, SWIFT_ROW_MAJOR, plan ? plan->p.M : 0, X, ldx,
+                     SWIFT_ROW_MAJOR, plan ? plan->p.K : 0));
+  Plan &p = const_cast<Plan &>(plan->p);
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  cudaStream_t st = S(stream);
+  SW_TRY(ensure_bwd(p, st));
+  if (p.K == 0 || N == 0) return SWIFT_OK;
+  DenseArgs d;
+  d.N = N; d.dtype = dtype; d.B = Y; d.ldb = ldy; d.C = X; d.ldc = ldx;
+  return run_rowwise(p, p.bwd, d, st);
+}
+
+swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const void *U,
+                         int64_t ldu, const void *V, int64_t ldv, void *out,
+                         swift_stream_t stream) {
+  SW_TRY(check_dense(plan, N, dtype, V, ldv, SWIFT_ROW_MAJOR, plan ? plan->p.K : 0, U, ldu,
+                     SWIFT_ROW_MAJOR, plan ? plan->p.M : 0));
+  Plan &p = const_cast<Plan &>(plan->p);
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  if (p.nnz > 0 && !out) return SWIFT_ERR_INVALID_ARG;
+  if (p.nnz == 0) return SWIFT_OK;
+  cudaStream_t st = S(stream);
+  if (N == 0) {
+    SW_CHECK_CUDA(cudaMemsetAsync(out, 0, p.vsz * (size_t)p.nnz, st));
+    return SWIFT_OK;
+  }
+  return run_sddmm(p, N, dtype, U, ldu, V, ldv, out, st);
+}
+
+swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_dtype dtype,
+                                          const void *X, int64_t ldx, const void *dY,
+                                          int64_t lddy, void *Y, int64_t ldy, void *dX,
+                                          int64_t lddx, void *dA, swift_stream_t stream) {
+  if (!plan || !X || !dY) return SWIFT_ERR_INVALID_ARG;
+  Plan &p = const_cast<Plan &>(plan->p);
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  if (dtype != SWIFT_F32 && dtype != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+  SW_TRY(check_dense(plan, N, dtype, X, ldx, SWIFT_ROW_MAJOR, p.K, dY, lddy, SWIFT_ROW_MAJOR, p.M));
+  cudaStream_t st = S(stream);
+  if (N == 0) return SWIFT_OK;
+  if (Y || dA) {
+    if (Y && dA) SW_TRY(run_fused_fwd_sddmm(p, N, dtype, X, ldx, dY, lddy, Y, ldy, dA, st));
+    else if (Y) {
+      DenseArgs d;
+      d.N = N; d.dtype = dtype; d.B = X; d.ldb = ldx; d.C = Y; d.ldc = ldy;
+      SW_TRY(run_rowwise(p, p.fwd, d, st));
+    } else SW_TRY(run_sddmm(p, N, dtype, dY, lddy, X, ldx, dA, st));
+  }
+  if (dX) {
+    SW_TRY(ensure_bwd(p, st));
+    DenseArgs d;
+    d.N = N; d.dtype = dtype; d.B = dY; d.ldb = lddy; d.C = dX; d.ldc = lddx;
+    SW_TRY(run_rowwise(p, p.bwd, d, st));
+  }
+  return SWIFT_OK;
+}
+
+swift_status swift_spmm_f64_reference(const swift_plan *plan, int N, const double *B,
+                                      int64_t ldb, double *C, int64_t ldc,
+                                      swift_stream_t stream) {
+  if (!plan || N < 0 || (N > 0 && (!B || !C)) || ldb < N || ldc < N) return SWIFT_ERR_INVALID_ARG;
+  return run_f64_reference(plan->p, N, B, ldb, C, ldc, S(stream));
+}
+
+swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, const void *B,
+                                 void *C, swift_stream_t stream, double *best_ms,
+                                 swift_engine *best_engine) {
+  if (!plan || !B || !C || N <= 0) return SWIFT_ERR_INVALID_ARG;
+  Plan &p = plan->p;
+  cudaStream_t st = S(stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best = 1e300;
+  swift_engine win = SWIFT_ENGINE_TILED;
+  const swift_engine cands[2] = {SWIFT_ENGINE_TILED, SWIFT_ENGINE_ROWWISE};
+  for (swift_engine eng : cands) {
+    if (eng == SWIFT_ENGINE_ROWWISE && !p.has_csr) continue;
+    if (eng == SWIFT_ENGINE_TILED && (dtype == SWIFT_BF16 || dtype == SWIFT_F16)) continue;
+    swift_status rc = SWIFT_OK;
+    for (int w = 0; w < 2 && rc == SWIFT_OK; ++w)
+      rc = swift_spmm(plan, eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
+    if (rc != SWIFT_OK) continue;
+    const int reps = 5;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps; ++r)
+      swift_spmm(plan, eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms / reps < best) { best = ms / reps; win = eng; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best >= 1e300) return SWIFT_ERR_UNSUPPORTED;
+  {
+    std::lock_guard<std::mutex> g(p.mu);
+    p.tuned[{N, (int)dtype}] = win;
+  }
+  if (best_ms) *best_ms = best;
+  if (best_engine) *best_engine = win;
+  return SWIFT_OK;
+}
+
+}  // extern "C"

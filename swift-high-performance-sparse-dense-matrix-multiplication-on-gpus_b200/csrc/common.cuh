@@ -1,0 +1,238 @@
+// common.cuh -- internal declarations shared by the Swift B200 library's translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "swift_b200.h"
+
+namespace swift {
+
+constexpr int kTile = 32;  // slidesize / TILESIZE of the reference (src/format.h:76-78)
+
+// ---------------------------------------------------------------- errors
+void set_last_error(const char *where, const char *what);
+
+#define SW_CHECK_CUDA(expr)                                                                  \
+  do {                                                                                       \
+    cudaError_t e__ = (expr);                                                                \
+    if (e__ != cudaSuccess) {                                                                \
+      ::swift::set_last_error(#expr, cudaGetErrorString(e__));                               \
+      return e__ == cudaErrorMemoryAllocation ? SWIFT_ERR_ALLOC : SWIFT_ERR_CUDA;            \
+    }                                                                                        \
+  } while (0)
+
+#define SW_CHECK_LAUNCH() SW_CHECK_CUDA(cudaGetLastError())
+
+#define SW_TRY(expr)                                                                         \
+  do {                                                                                       \
+    swift_status s__ = (expr);                                                               \
+    if (s__ != SWIFT_OK) return s__;                                                         \
+  } while (0)
+
+inline cudaStream_t S(swift_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------- device buffers
+// Owning device allocation (plan lifetime).  Size in bytes; never shared.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) { reset(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+    return *this;
+  }
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  swift_status alloc(size_t n) {
+    reset();
+    if (n == 0) n = 16;  // keep every pointer valid and 16-byte aligned
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_last_error("cudaMalloc", cudaGetErrorString(e));
+      return SWIFT_ERR_ALLOC;
+    }
+    bytes = n;
+    return SWIFT_OK;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Stream-ordered temporary (cudaMallocAsync / cudaFreeAsync on the same stream), so it may
+// go out of scope while kernels that use it are still queued.
+struct TmpBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  TmpBuf() = default;
+  TmpBuf(const TmpBuf &) = delete;
+  TmpBuf &operator=(const TmpBuf &) = delete;
+  ~TmpBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  swift_status alloc(size_t n, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    st = s;
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMallocAsync(&p, n, s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      set_last_error("cudaMallocAsync", cudaGetErrorString(e));
+      return SWIFT_ERR_ALLOC;
+    }
+    return SWIFT_OK;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------- plan
+struct RowLayout {
+  // Row-ordered execution of a CSR-shaped operand (A itself, or A^T = the sorted CSC).
+  int rows = 0, cols = 0, nnz = 0;
+  const int *ptr = nullptr;     // rows+1 (points into a plan buffer)
+  const int *idx = nullptr;     // nnz column (gather) indices
+  const void *val = nullptr;    // nnz values
+  const int *out_row = nullptr; // optional: output row of layout row r (NULL = r)
+  // long rows: rows with more than `split` nonzeros are cut into pieces of `split`
+  int split = 128;
+  int long_rows = 0, pieces = 0;
+  DevBuf piece_row;      // [pieces] layout row of each piece
+  DevBuf piece_idx;      // [pieces] index of the piece within its row
+  DevBuf long_first;     // [long_rows] first scratch slot / piece of each long row
+  DevBuf long_count;     // [long_rows] pieces of each long row
+  DevBuf long_of_row;    // [rows] long-row ordinal or -1
+  DevBuf counters;       // [long_rows] arrival counters (self-resetting)
+  DevBuf scratch;        // partial sums, grown on demand: pieces * N * 8 bytes
+  size_t scratch_bytes = 0;
+  bool built = false;
+};
+
+struct Plan {
+  int M = 0, K = 0, nnz = 0;
+  int device = 0;
+  int sm_count = 148;
+  swift_dtype val_type = SWIFT_F32;
+  size_t vsz = 4;  // bytes per value
+  bool has_csr = false;  // false for plans made from a host slide_matrix (compat path)
+
+  // CSR copy
+  DevBuf rowptr, colidx, val;
+  // column sort
+  DevBuf cnt;       // [K] nonzeros per original column
+  DevBuf perm;      // [K] sorted position -> original column
+  DevBuf invperm;   // [K]
+  DevBuf sortnnz;   // [K+1] counts in sorted order
+  DevBuf sptr;      // [K+1] sorted CSC pointer
+  DevBuf srow;      // [nnz] sorted CSC row indices
+  DevBuf sval;      // [nnz] sorted CSC values
+  DevBuf spos;      // [nnz] CSR position of each sorted CSC entry
+  // steps
+  int nsteps = 0;
+  DevBuf step_col, step_base, step_tall;  // [nsteps]
+  DevBuf step_tile_off;                   // [nsteps+1] first tile of each step
+  // regular tiles
+  int tilenum = 0;
+  int nstrips = 0;     // tiled-engine work items
+  DevBuf item_tile;    // [nstrips+1] first tile of each work item
+  DevBuf tile_colidx, tile_depth, tile_tall, tile_format;  // [tilenum]
+  DevBuf sortrowidx, sortval;                              // [32*tilenum]
+  int fmt_count[3] = {0, 0, 0};
+  // reside
+  int reside_col = 0, reside_nnz = 0;
+  DevBuf reside_ptr, reside_row, reside_val;  // [reside_col+1], [reside_nnz]
+  int numblk = 0;
+  DevBuf colorblk, blkstart, blkstop, blkptr;
+  // stats
+  int max_col = 0, max_row = 0, empty_cols = 0;
+  double build_ms = 0;
+  // row-ordered layouts
+  RowLayout fwd;  // A
+  RowLayout bwd;  // A^T (sorted CSC rows, output through perm)
+  int long_row_split = 128;
+  // autotuned choice per (N, dtype)
+  std::map<std::pair<int, int>, swift_engine> tuned;
+  std::mutex mu;  // guards lazily built layouts and scratch growth
+};
+
+size_t plan_device_bytes(const Plan &p);
+
+// ---------------------------------------------------------------- primitives (primitives.cu)
+// Exclusive scan of n int32 values into out (n+1 entries: out[n] = total).  `in` may alias
+// `out`.  Scratch is allocated stream-ordered.
+swift_status scan_exclusive_i32(const int *in, int *out, int64_t n, cudaStream_t st);
+// Stable LSD radix sort of (key, value) pairs by the low `bits` bits of key.  Results in
+// keys_out / vals_out.  keys_in / vals_in are clobbered.
+swift_status radix_sort_pairs(uint32_t *keys_in, uint32_t *vals_in, uint32_t *keys_out,
+                              uint32_t *vals_out, int64_t n, int bits, cudaStream_t st);
+// max over n int32 (n >= 0) into *dev_out (single int on device)
+swift_status reduce_max_i32(const int *in, int64_t n, int *dev_out, cudaStream_t st);
+
+// ---------------------------------------------------------------- format build (format_build.cu)
+swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *opts,
+                            cudaStream_t st);
+// Steps, tiles, reside and balance from a device-resident sorted CSC already in the plan
+// (p.sortnnz, p.sptr, p.srow, p.sval).
+swift_status build_tiles(Plan &p, cudaStream_t st);
+// Tiled-engine work items from tile_colidx (also used for plans made from a slide_matrix).
+swift_status build_items(Plan &p, cudaStream_t st);
+swift_status build_row_layout(Plan &p, RowLayout &L, bool transpose, cudaStream_t st);
+// Segment arrays of block_catgory on device (countrow[tilenum+1], segmentoffset[segsum+1],
+// sortrowindex[32*tilenum]); segsum returned on host.
+swift_status build_segments(const Plan &p, DevBuf &countrow, DevBuf &segmentoffset,
+                            DevBuf &sortrowindex, int *segsum, cudaStream_t st);
+// Per-8-tile row sort (back_process.h) on device into separate arrays.
+swift_status build_row_sort(const Plan &p, DevBuf &sorted_rows, DevBuf &val_position,
+                            DevBuf &val_offset, float *blockratio, cudaStream_t st);
+
+// ---------------------------------------------------------------- kernels (spmm_*.cu)
+struct DenseArgs {
+  int N = 0;
+  swift_dtype dtype = SWIFT_F32;
+  const void *B = nullptr;
+  int64_t ldb = 0;
+  swift_layout b_layout = SWIFT_ROW_MAJOR;
+  bool b_presorted = false;
+  void *C = nullptr;
+  int64_t ldc = 0;
+  swift_layout c_layout = SWIFT_ROW_MAJOR;
+};
+// variant 1 = reside per column without balance blocks (Swift_gpu1's kernel)
+swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cudaStream_t st);
+swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &a, cudaStream_t st);
+swift_status run_f64_reference(const Plan &p, int N, const double *B, int64_t ldb, double *C,
+                               int64_t ldc, cudaStream_t st);
+swift_status run_sddmm(Plan &p, int N, swift_dtype dt, const void *U, int64_t ldu,
+                       const void *V, int64_t ldv, void *out, cudaStream_t st);
+swift_status run_fused_fwd_sddmm(Plan &p, int N, swift_dtype dt, const void *X, int64_t ldx,
+                                 const void *dY, int64_t lddy, void *Y, int64_t ldy, void *dA,
+                                 cudaStream_t st);
+swift_status zero_dense(void *C, int rows, int N, int64_t ld, swift_layout layout, size_t esz,
+                        cudaStream_t st);
+
+// ---------------------------------------------------------------- device helpers
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+}  // namespace swift

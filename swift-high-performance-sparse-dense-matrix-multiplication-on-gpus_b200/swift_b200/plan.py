@@ -1,0 +1,257 @@
+"""Python view of a Swift plan (thin layer over the C ABI; device memory comes from torch).
+
+    plan = Plan.from_csr(rowptr, colidx, val, (M, K))   # numpy (host) or CUDA tensors
+    C = plan.spmm(B)                                     # C = A @ B on the current stream
+    X = plan.spmm_t(Y)                                   # A^T @ Y
+    dA = plan.sddmm(dY, X)                               # dY[row_e] . X[col_e] per nonzero
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi as capi
+
+_DT = {}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dtype_code(t):
+    torch = _torch()
+    m = {torch.float32: capi.F32, torch.float64: capi.F64, torch.bfloat16: capi.BF16, torch.float16: capi.F16}
+    if t not in m:
+        raise TypeError(f"unsupported dtype {t}")
+    return m[t]
+
+
+def _stream_ptr(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ld(t, layout):
+    if t.dim() != 2:
+        raise ValueError("dense operands are 2-D")
+    if layout == capi.ROW_MAJOR:
+        if t.stride(1) != 1:
+            raise ValueError("row-major operand needs unit column stride")
+        return t.stride(0)
+    if t.stride(0) != 1:
+        raise ValueError("column-major operand needs unit row stride")
+    return t.stride(1)
+
+
+class Plan:
+    """A Swift format resident on the current CUDA device."""
+
+    def __init__(self, handle, M, K, nnz, val_dtype, keep):
+        self._h = handle
+        self.M, self.K, self.nnz = M, K, nnz
+        self.val_dtype = val_dtype  # numpy dtype of A's values
+        self._keep = keep
+
+    # ------------------------------------------------------------------ construction
+    @classmethod
+    def from_csr(cls, rowptr, colidx, val, shape, col_perm=None, long_row_split=0,
+                 build_transpose=False, stream=None):
+        torch = _torch()
+        M, K = int(shape[0]), int(shape[1])
+        keep = []
+        on_dev = isinstance(rowptr, torch.Tensor) and rowptr.is_cuda
+        if on_dev:
+            rp = rowptr.to(torch.int32).contiguous()
+            ci = colidx.to(torch.int32).contiguous()
+            vv = val.contiguous()
+            if vv.dtype not in (torch.float32, torch.float64):
+                raise TypeError("A values must be float32 or float64")
+            keep += [rp, ci, vv]
+            ptrs = (rp.data_ptr(), ci.data_ptr(), vv.data_ptr())
+            vt = capi.F64 if vv.dtype == torch.float64 else capi.F32
+            nnz = int(ci.numel())
+            mem = capi.DEVICE
+            vdt = np.float64 if vt == capi.F64 else np.float32
+        else:
+            rp = np.ascontiguousarray(rowptr, np.int32)
+            ci = np.ascontiguousarray(colidx, np.int32)
+            vdt = np.float64 if np.asarray(val).dtype == np.float64 else np.float32
+            vv = np.ascontiguousarray(val, vdt)
+            keep += [rp, ci, vv]
+            ptrs = (rp.ctypes.data, ci.ctypes.data if ci.size else rp.ctypes.data,
+                    vv.ctypes.data if vv.size else rp.ctypes.data)
+            vt = capi.F64 if vdt == np.float64 else capi.F32
+            nnz = int(ci.size)
+            mem = capi.HOST
+        a = capi.swift_csr(M, K, nnz, ptrs[0], ptrs[1], ptrs[2], vt, mem)
+        o = capi.swift_plan_opts()
+        o.long_row_split = int(long_row_split)
+        o.build_transpose = int(bool(build_transpose))
+        if col_perm is not None:
+            if isinstance(col_perm, torch.Tensor) and col_perm.is_cuda:
+                cp = col_perm.to(torch.int32).contiguous()
+                o.col_perm, o.col_perm_mem = cp.data_ptr(), capi.DEVICE
+            else:
+                cp = np.ascontiguousarray(col_perm, np.int32)
+                o.col_perm, o.col_perm_mem = cp.ctypes.data, capi.HOST
+            keep.append(cp)
+        h = C.c_void_p()
+        capi.check(capi.lib().swift_plan_create(C.byref(a), C.byref(o), _stream_ptr(stream), C.byref(h)),
+                   "swift_plan_create")
+        return cls(h, M, K, nnz, vdt, [] if not on_dev else keep)
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            capi.lib().swift_plan_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------------ introspection
+    def stats(self) -> dict:
+        s = capi.swift_plan_stats()
+        capi.check(capi.lib().swift_plan_get_stats(self._h, C.byref(s)), "swift_plan_get_stats")
+        d = {k: getattr(s, k) for k, _ in s._fields_}
+        d["fmt_count"] = list(s.fmt_count)
+        return d
+
+    def export(self, with_row_sort=False) -> dict:
+        """Every reference slide_matrix array as numpy (host copies made on the GPU)."""
+        f64 = self.val_dtype == np.float64
+        S = capi.swift_slide_matrix_f64 if f64 else capi.swift_slide_matrix_f32
+        s = S()
+        br = C.c_float(0)
+        fn = capi.lib().swift_plan_export_f64 if f64 else capi.lib().swift_plan_export_f32
+        capi.check(fn(self._h, C.byref(s), int(with_row_sort), C.byref(br)), "swift_plan_export")
+        vdt = np.float64 if f64 else np.float32
+
+        def arr(ptr, n, dt):
+            if n <= 0 or not ptr:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
+
+        T, R, RC, RN, NB = s.tilenum, s.regular_nnz, s.reside_col, s.reside_nnz, s.numblk
+        out = dict(tilenum=T, regular_nnz=R, reside_col=RC, reside_nnz=RN, numblk=NB, segsum=s.segsum)
+        out["tile_ptr"] = arr(s.tile_ptr, T + 1, np.int32)
+        out["tile_len"] = arr(s.tile_len, T, np.int32)
+        out["tile_colidx"] = arr(s.tile_colidx, T, np.int32)
+        out["tile_tall"] = arr(s.tile_tall, T, np.int32)
+        out["tile_format"] = arr(s.tile_format, T, np.int32)
+        out["sortrowidx"] = arr(s.sortrowidx, R, np.int32)
+        out["sortval"] = arr(s.sortval, R, vdt)
+        out["countrow"] = arr(s.countrow, T + 1, np.int32)
+        out["segmentoffset"] = arr(s.segmentoffset, s.segsum + 1, np.int32)
+        out["sortrowindex"] = arr(s.sortrowindex, R, np.int32)
+        out["reside_cscptr"] = arr(s.reside_cscptr, RC + 1, np.int32)
+        out["reside_cscrowidx"] = arr(s.reside_cscrowidx, RN, np.int32)
+        out["reside_val"] = arr(s.reside_val, RN, vdt)
+        out["colorblk"] = arr(s.colorblk, NB, np.uint32)
+        out["blkstart"] = arr(s.blkstart, NB, np.int32)
+        out["blkstop"] = arr(s.blkstop, NB, np.int32)
+        out["blkptr"] = arr(s.blkptr, NB, np.int32)
+        if with_row_sort:
+            out["val_position"] = arr(s.val_position, R, np.int32)
+            out["val_offset"] = arr(s.val_offset, R, np.int32)
+            out["blockratio"] = np.float32(br.value)
+        (capi.lib().swift_slide_free_f64 if f64 else capi.lib().swift_slide_free_f32)(C.byref(s))
+        return out
+
+    def export_sorted(self):
+        """(perm, sortnnz, sorted CSC row indices, sorted CSC values) as numpy."""
+        perm = np.zeros(max(self.K, 1), np.int32)
+        sn = np.zeros(max(self.K, 1), np.int32)
+        sr = np.zeros(max(self.nnz, 1), np.int32)
+        sv = np.zeros(max(self.nnz, 1), self.val_dtype)
+        capi.check(capi.lib().swift_plan_export_sorted(self._h, perm.ctypes.data, sn.ctypes.data,
+                                                        sr.ctypes.data, sv.ctypes.data),
+                   "swift_plan_export_sorted")
+        return perm[:self.K], sn[:self.K], sr[:self.nnz], sv[:self.nnz]
+
+    # ------------------------------------------------------------------ products
+    def spmm(self, B, C_out=None, engine="auto", b_presorted=False, layout="row", stream=None):
+        """C = A @ B.  layout 'row' (row-major B/C) or 'col' (column-major, Fortran order)."""
+        torch = _torch()
+        lay = capi.ROW_MAJOR if layout == "row" else capi.COL_MAJOR
+        N = int(B.shape[1])
+        if C_out is None:
+            C_out = torch.empty((self.M, N), dtype=B.dtype, device=B.device)
+            if lay == capi.COL_MAJOR:
+                C_out = torch.empty((N, self.M), dtype=B.dtype, device=B.device).t()
+        eng = {"auto": capi.ENGINE_AUTO, "tiled": capi.ENGINE_TILED, "rowwise": capi.ENGINE_ROWWISE}[engine]
+        capi.check(capi.lib().swift_spmm(self._h, eng, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, lay), lay,
+                                         int(b_presorted), C_out.data_ptr(), _ld(C_out, lay), lay,
+                                         _stream_ptr(stream)), "swift_spmm")
+        return C_out
+
+    def spmm_t(self, Y, X_out=None, stream=None):
+        """X = A^T @ Y (row-major)."""
+        torch = _torch()
+        N = int(Y.shape[1])
+        if X_out is None:
+            X_out = torch.empty((self.K, N), dtype=Y.dtype, device=Y.device)
+        capi.check(capi.lib().swift_spmm_transposed(self._h, N, _dtype_code(Y.dtype), Y.data_ptr(),
+                                                    _ld(Y, 0), X_out.data_ptr(), _ld(X_out, 0),
+                                                    _stream_ptr(stream)), "swift_spmm_transposed")
+        return X_out
+
+    def sddmm(self, U, V, out=None, stream=None):
+        """out[e] = U[row_e] . V[col_e] for every nonzero e in CSR order."""
+        torch = _torch()
+        N = int(U.shape[1])
+        vt = torch.float64 if self.val_dtype == np.float64 else torch.float32
+        if out is None:
+            out = torch.empty(self.nnz, dtype=vt, device=U.device)
+        capi.check(capi.lib().swift_sddmm(self._h, N, _dtype_code(U.dtype), U.data_ptr(), _ld(U, 0),
+                                          V.data_ptr(), _ld(V, 0), out.data_ptr(), _stream_ptr(stream)),
+                   "swift_sddmm")
+        return out
+
+    def fused_forward_backward(self, X, dY, Y=None, dX=None, dA=None, want=("Y", "dX", "dA"), stream=None):
+        torch = _torch()
+        N = int(X.shape[1])
+        if "Y" in want and Y is None:
+            Y = torch.empty((self.M, N), dtype=X.dtype, device=X.device)
+        if "dX" in want and dX is None:
+            dX = torch.empty((self.K, N), dtype=X.dtype, device=X.device)
+        if "dA" in want and dA is None:
+            dA = torch.empty(self.nnz, dtype=X.dtype, device=X.device)
+
+        def p(t):
+            return t.data_ptr() if t is not None else None
+
+        def ld(t):
+            return _ld(t, 0) if t is not None else 0
+        capi.check(capi.lib().swift_fused_forward_backward(
+            self._h, N, _dtype_code(X.dtype), X.data_ptr(), ld(X), dY.data_ptr(), ld(dY), p(Y), ld(Y),
+            p(dX), ld(dX), p(dA), _stream_ptr(stream)), "swift_fused_forward_backward")
+        return Y, dX, dA
+
+    def spmm_f64_reference(self, B64, stream=None):
+        torch = _torch()
+        N = int(B64.shape[1])
+        out = torch.empty((self.M, N), dtype=torch.float64, device=B64.device)
+        capi.check(capi.lib().swift_spmm_f64_reference(self._h, N, B64.data_ptr(), _ld(B64, 0),
+                                                       out.data_ptr(), _ld(out, 0), _stream_ptr(stream)),
+                   "swift_spmm_f64_reference")
+        return out
+
+    def autotune(self, B, C_out, stream=None):
+        ms = C.c_double(0)
+        eng = C.c_int(0)
+        N = int(B.shape[1])
+        capi.check(capi.lib().swift_plan_autotune(self._h, N, _dtype_code(B.dtype), B.data_ptr(),
+                                                  C_out.data_ptr(), _stream_ptr(stream), C.byref(ms),
+                                                  C.byref(eng)), "swift_plan_autotune")
+        return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise"}[eng.value], ms.value

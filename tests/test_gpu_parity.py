@@ -1,0 +1,205 @@
+"""GPU parity: the CUDA library (called through its C ABI) against the reference.
+
+* Format arrays built on the GPU are bit-exact with the reference's preprocessing (committed
+  fixtures made by the reference's own code, and the oracle on further cases).
+* C matches the reference's Swift_cpu: normwise max|C - C_ref| / max|C_ref| <= 1e-5 (FP32),
+  <= 1e-12 (FP64); the error against the deterministic FP64 GPU product is checked beside it.
+"""
+import numpy as np
+import pytest
+
+import cases
+import golden_io
+import oracle
+from swift_b200 import Plan, gen
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float32: 1e-5, np.float64: 1e-12}
+
+
+def relerr(x, ref):
+    x = np.asarray(x, np.float64)
+    ref = np.asarray(ref, np.float64)
+    d = max(np.abs(ref).max(), 1e-300) if ref.size else 1.0
+    return float(np.abs(x - ref).max() / d) if ref.size else 0.0
+
+
+def plan_of(g, dt):
+    return Plan.from_csr(g["rowptr"], g["colidx"], g["val"].astype(dt), (g["M"], g["K"]))
+
+
+def tdev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("name", golden_io.ALL)
+def test_format_bit_exact_vs_reference_fixture(name, dt):
+    g = golden_io.load(name, dt)
+    pl = plan_of(g, dt)
+    ex = pl.export(with_row_sort=True)
+    for k in golden_io.SCALARS:
+        if k == "nsteps":
+            assert pl.stats()["nsteps"] == g[k]
+        else:
+            assert ex[k] == g[k], k
+    for k in golden_io.ARRAYS:
+        if k in ("val_position", "rowsorted_rowidx", "sortrowidx"):
+            continue
+        assert np.array_equal(ex[k], g[k].astype(ex[k].dtype)), k
+    # export with the row sort overwrites sortrowidx with sorted keys, as the reference does
+    assert np.array_equal(ex["sortrowidx"], g["rowsorted_rowidx"])
+    nr = ex["regular_nnz"]
+    for g0 in range(0, nr, 256):
+        g1 = min(g0 + 256, nr)
+        p = ex["val_position"][g0:g1]
+        assert np.array_equal(np.sort(p), np.arange(g1 - g0))
+        assert np.array_equal(g["rowsorted_rowidx"][g0:g1][p], g["sortrowidx"][g0:g1])
+    perm, sn, sr, sv = pl.export_sorted()
+    assert np.array_equal(perm, g["perm"]) and np.array_equal(sn, g["sortnnz"])
+    ex2 = pl.export(with_row_sort=False)
+    assert np.array_equal(ex2["sortrowidx"], g["sortrowidx"])
+    pl.close()
+
+
+@pytest.mark.parametrize("engine", ["tiled", "rowwise"])
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("name", golden_io.ALL)
+def test_spmm_matches_swift_cpu(name, dt, engine):
+    g = golden_io.load(name, dt)
+    pl = plan_of(g, dt)
+    B = tdev(g["B"])
+    Cm = pl.spmm(B, engine=engine).cpu().numpy()
+    assert Cm.dtype == dt
+    assert relerr(Cm, g["C"]) <= TOL[dt], relerr(Cm, g["C"])
+    c64 = pl.spmm_f64_reference(B.double()).cpu().numpy()
+    assert relerr(c64, oracle.csr_spmm_f64(g["M"], g["K"], g["rowptr"], g["colidx"], g["val"], g["B"])) <= 1e-14
+    assert relerr(Cm, c64) <= TOL[dt]
+    pl.close()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("name", ["poisson4096", "long_col", "same_rows", "k_mod_31"])
+def test_tiled_colmajor_presorted_like_reference_wrappers(name, dt):
+    """The reference wrappers take the column-sorted B in column-major order and return C
+    column-major (src/main.cu:338-340, src/Swift.h:390-396)."""
+    g = golden_io.load(name, dt)
+    pl = plan_of(g, dt)
+    sortB = g["B"][g["perm"]]
+    Bcm = torch.from_numpy(np.asfortranarray(sortB)).cuda().t().contiguous().t()  # column-major view
+    assert Bcm.stride(0) == 1
+    Cm = pl.spmm(Bcm, engine="tiled", b_presorted=True, layout="col").cpu().numpy()
+    assert relerr(Cm, g["C"]) <= TOL[dt]
+    # unsorted B, column-major, perm applied on the fly
+    Bcm2 = torch.from_numpy(np.asfortranarray(g["B"])).cuda().t().contiguous().t()
+    Cm2 = pl.spmm(Bcm2, engine="tiled", layout="col").cpu().numpy()
+    assert relerr(Cm2, g["C"]) <= TOL[dt]
+    pl.close()
+
+
+@pytest.mark.parametrize("N", [1, 8, 24, 32, 33, 64, 128, 768])
+@pytest.mark.parametrize("engine", ["tiled", "rowwise"])
+def test_ragged_widths(N, engine):
+    M, K, rp, ci = cases.make("rmat12", 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    Bn = gen.dense_uniform(K, N, 2, np.float32)
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, Bn)
+    pl = Plan.from_csr(rp, ci, val, (M, K), long_row_split=64)
+    Cm = pl.spmm(tdev(Bn), engine=engine).cpu().numpy()
+    assert relerr(Cm, ref) <= 1e-5
+    # strided operands (leading dimension > N)
+    Bp = torch.zeros((K, N + 3), dtype=torch.float32, device="cuda")
+    Bp[:, :N] = tdev(Bn)
+    Cp = torch.full((M, N + 5), 7.0, dtype=torch.float32, device="cuda")
+    pl.spmm(Bp[:, :N], Cp[:, :N], engine=engine)
+    assert relerr(Cp[:, :N].cpu().numpy(), ref) <= 1e-5
+    assert torch.all(Cp[:, N:] == 7.0)
+    pl.close()
+
+
+@pytest.mark.parametrize("split", [16, 32, 128, 100000])
+def test_long_row_split_is_deterministic(split):
+    M, K, rp, ci = cases.make("rmat12", 3)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    Bn = gen.dense_uniform(K, 128, 2, np.float32)
+    pl = Plan.from_csr(rp, ci, val, (M, K), long_row_split=split)
+    st = pl.stats()
+    if split < st["max_row_nnz"]:
+        assert st["long_rows"] > 0
+    B = tdev(Bn)
+    c1 = pl.spmm(B, engine="rowwise")
+    c2 = pl.spmm(B, engine="rowwise")
+    assert torch.equal(c1, c2)
+    assert relerr(c1.cpu().numpy(), oracle.csr_spmm_f64(M, K, rp, ci, val, Bn)) <= 1e-5
+    pl.close()
+
+
+@pytest.mark.parametrize("dt16", ["bf16", "f16"])
+def test_low_precision_operands(dt16):
+    M, K, rp, ci = cases.make("rmat12", 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    Bn = gen.dense_uniform(K, 128, 2, np.float32)
+    tdt = torch.bfloat16 if dt16 == "bf16" else torch.float16
+    B16 = tdev(Bn).to(tdt)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    C16 = pl.spmm(B16)
+    assert C16.dtype == tdt
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, B16.float().cpu().numpy().astype(np.float64))
+    assert relerr(C16.double().cpu().numpy(), ref) <= 1e-2
+    pl.close()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("name", ["rmat12", "skewed", "rect_wide", "rect_tall", "empty", "long_col"])
+def test_backward_products(name, dt):
+    M, K, rp, ci = cases.make(name, 0)
+    val = gen.uniform_values(int(rp[-1]), 1, dt)
+    N = 64
+    X = gen.dense_uniform(K, N, 5, dt)
+    dY = gen.dense_uniform(M, N, 6, dt)
+    pl = Plan.from_csr(rp, ci, val, (M, K), long_row_split=32)
+    tol = TOL[dt] * (10 if dt == np.float32 else 1)
+    dX = pl.spmm_t(tdev(dY)).cpu().numpy()
+    assert relerr(dX, oracle.csr_spmm_t_f64(M, K, rp, ci, val, dY)) <= tol
+    dA = pl.sddmm(tdev(dY), tdev(X)).cpu().numpy()
+    assert relerr(dA, oracle.sddmm_f64(M, K, rp, ci, dY, X)) <= tol
+    Y, dX2, dA2 = pl.fused_forward_backward(tdev(X), tdev(dY))
+    assert relerr(Y.cpu().numpy(), oracle.csr_spmm_f64(M, K, rp, ci, val, X)) <= tol
+    assert relerr(dX2.cpu().numpy(), oracle.csr_spmm_t_f64(M, K, rp, ci, val, dY)) <= tol
+    assert relerr(dA2.cpu().numpy(), oracle.sddmm_f64(M, K, rp, ci, dY, X)) <= tol
+    pl.close()
+
+
+def test_device_resident_csr_and_injected_perm():
+    g = golden_io.load("skewed")
+    r, p, cnt, v = oracle.csr2csc(g["M"], g["K"], g["rowptr"], g["colidx"], g["val"])
+    pm = oracle.perm_stable(cnt)[::-1].copy()  # not sorted -> must be rejected
+    with pytest.raises(Exception):
+        Plan.from_csr(g["rowptr"], g["colidx"], g["val"], (g["M"], g["K"]), col_perm=pm)
+    # a valid alternative order: ties reversed
+    keys = cnt.astype(np.int64) * g["K"] + (g["K"] - 1 - np.arange(g["K"]))
+    pm2 = np.argsort(keys, kind="stable").astype(np.int32)
+    pl = Plan.from_csr(tdev(g["rowptr"]), tdev(g["colidx"]), tdev(g["val"]), (g["M"], g["K"]), col_perm=pm2)
+    perm, *_ = pl.export_sorted()
+    assert np.array_equal(perm, pm2)
+    ref = oracle.pipeline(g["M"], g["K"], g["rowptr"], g["colidx"], g["val"], g["B"], perm=pm2)
+    ex = pl.export()
+    for k in ("sortrowidx", "sortval", "reside_cscrowidx", "reside_val", "tile_colidx", "colorblk"):
+        assert np.array_equal(ex[k], ref["slide"][k]), k
+    assert relerr(pl.spmm(tdev(g["B"]), engine="tiled").cpu().numpy(), ref["C"]) <= 1e-5
+    pl.close()
+
+
+def test_bad_csr_rejected():
+    from swift_b200 import capi
+    rp = np.array([0, 2, 1, 3], np.int32)
+    ci = np.array([0, 1, 2], np.int32)
+    with pytest.raises(capi.SwiftError) as e:
+        Plan.from_csr(rp, ci, np.ones(3, np.float32), (3, 3))
+    assert e.value.status == capi.ERR_BAD_CSR
+    rp = np.array([0, 1, 2, 3], np.int32)
+    ci = np.array([0, 1, 9], np.int32)
+    with pytest.raises(capi.SwiftError):
+        Plan.from_csr(tdev(rp), tdev(ci), tdev(np.ones(3, np.float32)), (3, 3))
