@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Swift SpMM benchmark (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+A step is one product C = A B over the workload (default: the 1,048,576 x 1,048,576 R-MAT
+matrix, a,b,c,d = .57,.19,.19,.05, 16,777,216 edge draws with duplicates merged, values
+U[-1,1] FP32, B 1,048,576 x 128 FP32 U[-1,1]).  `value` is whole-job GFLOP/s (2 nnz N per
+step, summed over ranks) with A, B and C resident in HBM; `e2e` is the same metric through the
+library's public call with B copied in from pinned host memory and C copied back every step.
+Several GPUs run independent replicas (the product has no exchange step).
+
+--impl reference times the reference's own CPU product (Swift_cpu, compiled from the
+reference sources under oracle/_ref; the oracle's restatement if that build is absent) on
+the host cores: each step is a bounded sample of tiles of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "swift-high-performance-sparse-dense-matrix-multiplication-on-gpus_b200")
+sys.path[:0] = [PKG_DIR, os.path.join(ROOT, "oracle")]
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # the scale workloads (R-MAT scale 20, avg degree 16)
+    "rmat20_n128_f32": dict(kind="rmat", scale=20, edges=16 << 20, N=128, dtype="f32"),
+    "rmat20_n32_f32": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f32"),
+    "rmat20_n128_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=128, dtype="f64"),
+    "rmat20_n32_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f64"),
+    # precision workload: R-MAT scale 19 avg degree 32 merged with a 64-wide band, 16-bit B/C
+    "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
+    "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),
+    "rmat19band_n128_f32": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f32"),
+    # the 4096 x 4096 parity workload (rows ~Poisson(16))
+    "poisson4096_n32_f32": dict(kind="poisson", M=4096, K=4096, lam=16.0, N=32, dtype="f32"),
+}
+DEFAULT_WORKLOAD = "rmat20_n128_f32"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def describe(name, wl, nnz):
+    if wl["kind"] == "rmat":
+        M = 1 << wl["scale"]
+        return (f"R-MAT scale {wl['scale']} ({M}x{M}, {wl['edges']} edge draws, a,b,c,d=.57,.19,.19,.05, "
+                f"duplicates merged -> {nnz} nnz), values U[-1,1]; B {M}x{wl['N']} U[-1,1] row-major; "
+                f"C = A*B {wl['dtype']}")
+    if wl["kind"] == "rmatband":
+        M = 1 << wl["scale"]
+        return (f"R-MAT scale {wl['scale']} ({wl['edges']} draws) merged with |i-j|<32 band -> {nnz} nnz, "
+                f"values U[-1,1] FP32; B {M}x{wl['N']} and C in {wl['dtype']}, FP32 accumulation")
+    return (f"{wl['M']}x{wl['K']} rows ~Poisson({wl['lam']}), columns uniform without replacement -> "
+            f"{nnz} nnz; B {wl['K']}x{wl['N']} U[-1,1]")
+
+
+def make_inputs(wl, device, seed=0):
+    """Pattern and values (host numpy CSR) plus B on `device` (torch)."""
+    import torch
+
+    from swift_b200 import gen
+    if wl["kind"] == "rmat":
+        rp, ci = gen.rmat(wl["scale"], wl["edges"], seed=seed, device=device)
+        M = K = 1 << wl["scale"]
+    elif wl["kind"] == "rmatband":
+        rp, ci = gen.rmat_plus_band(wl["scale"], wl["edges"], 32, seed=seed, device=device)
+        M = K = 1 << wl["scale"]
+    else:
+        M, K = wl["M"], wl["K"]
+        rp, ci = gen.poisson_uniform(M, K, wl["lam"], seed=seed)
+    nnz = int(rp[-1])
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 1)
+    vdt = torch.float64 if wl["dtype"] == "f64" else torch.float32
+    val = (torch.rand(nnz, generator=g, device=device, dtype=vdt) * 2 - 1)
+    g.manual_seed(seed + 2)
+    if wl["dtype"] == "f64":
+        B = torch.rand((K, wl["N"]), generator=g, device=device, dtype=torch.float64) * 2 - 1
+    else:
+        bdt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[wl["dtype"]]
+        B = (torch.rand((K, wl["N"]), generator=g, device=device, dtype=torch.float32) * 2 - 1).to(bdt)
+    return M, K, rp, ci, val, B
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.lines = []
+        self.proc = None
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "50", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+        time.sleep(0.15)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self, t0, t1):
+        if self.proc is None:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        inside = [ln for ts, ln in self.lines if t0 - 0.06 <= ts <= t1 + 0.06] or [ln for _, ln in self.lines]
+        mhz, mx, reasons = [], None, set()
+        for ln in inside:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(self.NAMES, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not mhz:
+            return None
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profile(kernel, workload):
+    """dram bytes per launch from the committed ncu summary of this kernel and workload."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class _StdoutToStderr:
+    """Routes C-level stdout to stderr (the reference's host code prints progress and
+    diagnostic lines; stdout carries only the JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def cpu_swift(M, K, rp, ci, val_np, B_np, N, impl="ref"):
+    """The reference's host pipeline (csr2csc, col_sort, formattransation, block_catgory,
+    balance) and a Swift_cpu sampler over its format."""
+    with _StdoutToStderr():
+        return _cpu_swift(M, K, rp, ci, val_np, B_np, N, impl)
+
+
+def _cpu_swift(M, K, rp, ci, val_np, B_np, N, impl):
+    import oracle
+    dt = val_np.dtype.type
+    use = "ref" if (impl == "ref" and oracle.ref_available()) else "oracle"
+    r, p, cnt, v = oracle.csr2csc(M, K, rp, ci, val_np, impl=use)
+    pm = oracle.perm_stable(cnt)
+    sr, sv, sn, sB = oracle.col_sort(K, N, cnt, pm, p, r, v, B=B_np, impl=use)
+    del r, v
+    sl = oracle.build(sr, sv, sn, M, K, impl=use, row_sort=False)
+    return oracle.CpuSwift(sl, M, K, N, sB, impl=use), use
+
+
+def run_cpu_samples(cs, seconds, warm=1):
+    """Time consecutive tile ranges until `seconds` of CPU work; returns (GFLOP/s, sample)."""
+    T = cs.tilenum
+    chunk = max(1, min(T, 4096))
+    t = 0
+    for _ in range(warm):
+        cs.run(0, min(chunk, T))
+    tot_s, tot_nnz, ranges = 0.0, 0, 0
+    while tot_s < seconds and T > 0:
+        t1 = min(T, t + chunk)
+        s, n = cs.run(t, t1)
+        tot_s += s
+        tot_nnz += n
+        ranges += 1
+        t = 0 if t1 >= T else t1
+    gf = 2.0 * tot_nnz * cs.N / tot_s / 1e9 if tot_s > 0 else 0.0
+    return gf, tot_s, tot_nnz
+
+
+# ------------------------------------------------------------------------------------ ours
+def run_ours(args):
+    import torch
+
+    from swift_b200 import Plan
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    wl = WORKLOADS[args.workload]
+    N = wl["N"]
+    M, K, rp, ci, val, B = make_inputs(wl, "cuda")
+    nnz = int(rp[-1])
+    d_rp = torch.from_numpy(rp).cuda()
+    d_ci = torch.from_numpy(ci).cuda()
+    plan = Plan.from_csr(d_rp, d_ci, val, (M, K))
+    C = torch.empty((M, N), dtype=B.dtype, device="cuda")
+    engine, tune_ms = plan.autotune(B, C)
+    st = plan.stats()
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        plan.spmm(B, C)
+    gpu_idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[local] if os.environ.get("CUDA_VISIBLE_DEVICES") else local
+    sampler = ClockSampler(gpu_idx)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.spmm(B, C)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    clocks = sampler.stop(w0, w1)
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    flops = 2.0 * nnz * N
+    value = world * flops * args.steps / (ms / 1e3) / 1e9
+    esz = B.element_size()
+    vsz = 8 if val.dtype == torch.float64 else 4
+    alg_bytes = nnz * (vsz + 4) + K * N * esz + M * N * esz
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    kernel = "rowwise_kernel" if engine == "rowwise" else "tiled_rowmajor_kernel"
+    traffic = traffic_from_profile(kernel, args.workload)
+
+    # the Swift tiled engine on the same inputs (reported beside the chosen engine)
+    tiled = None
+    if B.dtype in (torch.float32, torch.float64):
+        for _ in range(2):
+            plan.spmm(B, C, engine="tiled")
+        n_t = 5
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(n_t):
+            plan.spmm(B, C, engine="tiled")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_ms = e0.elapsed_time(e1) / n_t
+        tiled = {"gflops": flops / (t_ms / 1e3) / 1e9, "ms_per_step": t_ms,
+                 "hbm_frac_of_measured": alg_bytes / (t_ms / 1e3) / 1e9 / peak}
+        plan.spmm(B, C)
+
+    # end to end: B from pinned host memory in, C back out, through the public call
+    Bh = B.cpu().pin_memory()
+    Ch = torch.empty((M, N), dtype=C.dtype).pin_memory()
+    for _ in range(1):
+        B.copy_(Bh, non_blocking=True)
+        plan.spmm(B, C)
+        Ch.copy_(C, non_blocking=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        B.copy_(Bh, non_blocking=True)
+        plan.spmm(B, C)
+        Ch.copy_(C, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * flops * args.e2e_steps / (e2e_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cs, kind = cpu_swift(M, K, rp, ci, val.cpu().numpy(),
+                                 B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy(),
+                                 N, impl="ref")
+            gf, secs, snnz = run_cpu_samples(cs, args.cpu_seconds)
+            cpu = {"value": gf, "unit": "GFLOP/s", "cores": 1,
+                   "kind": "reference" if kind == "ref" else "port",
+                   "sample": f"Swift_cpu over consecutive tile ranges of this workload: {snnz} nonzeros x N={N} "
+                             f"in {secs:.1f} s (single-threaded by construction; host has {os.cpu_count()} threads)"}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    dtype = wl["dtype"]
+    out = {
+        "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz),
+                   "rows": M, "cols": K, "nnz": nnz, "N": N, "engine": engine,
+                   "parallelism": f"replicas x{world} (no exchange step)",
+                   "l2": "inputs larger than L2 (B and C exceed 126 MB); no flush between steps",
+                   "plan_build_ms": st["build_ms"], "autotune_ms": tune_ms,
+                   "format": {k: st[k] for k in ("nsteps", "tilenum", "reside_col", "reside_nnz", "numblk",
+                                                  "fmt_count", "long_rows", "long_pieces", "max_row_nnz")}},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} ({'MEASURED_PEAKS.json hbm_gbs' if peak_kind == 'measured' else 'pool fallback'})",
+                     "kernel": kernel, "algorithmic_bytes_per_launch": alg_bytes,
+                     "frac_of_8TBs_nominal": achieved / 8000.0},
+        "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": int(Bh.numel() * Bh.element_size()),
+                "d2h_bytes_per_step": int(Ch.numel() * Ch.element_size()), "steps": args.e2e_steps,
+                "ms_per_step": e2e_ms / args.e2e_steps},
+        "gpu_launches": args.steps * (1 if engine == "rowwise" else 2),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "tiled_engine": tiled,
+    }
+    print(json.dumps(out), flush=True)
+    plan.close()
+
+
+# ------------------------------------------------------------------------------------ reference
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    N = wl["N"]
+    try:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+    except Exception:
+        dev = "cpu"
+    M, K, rp, ci, val, B = make_inputs(wl, dev)
+    import torch
+    Bn = B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy()
+    vn = val.cpu().numpy()
+    nnz = int(rp[-1])
+    cs, kind = cpu_swift(M, K, rp, ci, vn, Bn, N, impl="ref")
+    T = cs.tilenum
+    # size each step so that warmup + steps take about a minute of CPU time
+    s, n = cs.run(0, min(T, 256))
+    per_tile = s / max(1, min(T, 256))
+    budget = float(args.ref_seconds)
+    chunk = int(max(1, min(T, budget / max(1, args.steps + args.warmup) / max(per_tile, 1e-9))))
+    t = 0
+    for _ in range(args.warmup):
+        t1 = min(T, t + chunk)
+        cs.run(t, t1)
+        t = 0 if t1 >= T else t1
+    tot_s, tot_nnz = 0.0, 0
+    for _ in range(args.steps):
+        t1 = min(T, t + chunk)
+        sec, n = cs.run(t, t1)
+        tot_s += sec
+        tot_nnz += n
+        t = 0 if t1 >= T else t1
+    value = 2.0 * tot_nnz * N / tot_s / 1e9 if tot_s > 0 else 0.0
+    sample = (f"each step: Swift_cpu over {chunk} consecutive tiles ({chunk * 32} nonzeros x N={N}) of this workload; "
+              f"{tot_nnz} nonzeros in {tot_s:.2f} s over {args.steps} steps")
+    out = {
+        "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot_s * 1e3 / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"], "impl": "reference",
+        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
+                   "cols": K, "nnz": nnz, "N": N, "parallelism": "host CPU, rank 0 only"},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": 1,
+                         "kind": "reference" if kind == "ref" else "port", "sample": sample},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", type=float, default=60.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -319,3 +319,57 @@ def sddmm_f64(M, K, rowptr, colidx, U, V):
                                       _p(np.ascontiguousarray(colidx, np.int32)),
                                       _p(Uc, C.c_double), _p(Vc, C.c_double), _p(out, C.c_double))
     return out[:nnz]
+
+
+class CpuSwift:
+    """Swift_cpu held ready for repeated timed samples over tile ranges (CPU baseline).
+
+    ``impl="ref"`` runs the reference's own Swift_cpu (compiled from its checkout) on a view
+    of the format; ``impl="oracle"`` the restatement.  Both are single-threaded by
+    construction, as the reference is."""
+
+    def __init__(self, slide: Slide, M, K, N, sortB, impl="ref"):
+        self.dt = slide.dtype
+        self.impl = impl if (impl != "ref" or ref_available()) else "oracle"
+        self.M, self.K, self.N = M, K, N
+        self.tilenum = slide.tilenum
+        S = _SLIDE[self.dt]
+        self.s = S()
+        self._keep = []
+
+        def put(name, arr, ct=C.c_int):
+            a = np.ascontiguousarray(arr)
+            if a.size == 0:
+                a = np.zeros(1, a.dtype)
+            self._keep.append(a)
+            setattr(self.s, name, a.ctypes.data_as(C.POINTER(ct)))
+
+        self.s.tilenum, self.s.regular_nnz = slide.tilenum, slide.regular_nnz
+        self.s.reside_col, self.s.reside_nnz = slide.reside_col, slide.reside_nnz
+        put("tile_ptr", slide["tile_ptr"])
+        put("tile_len", slide["tile_len"])
+        put("tile_colidx", slide["tile_colidx"])
+        put("sortrowidx", slide["sortrowidx"])
+        put("sortval", slide["sortval"].astype(self.dt), _CT[self.dt])
+        put("reside_cscptr", slide["reside_cscptr"])
+        put("reside_cscrowidx", slide["reside_cscrowidx"])
+        put("reside_val", slide["reside_val"].astype(self.dt), _CT[self.dt])
+        self.sortB = np.ascontiguousarray(sortB, self.dt)
+        self.C = np.zeros((M, N), self.dt)
+        if self.impl == "ref":
+            self.fn = getattr(_lib("ref", self.dt), "ref_swift_cpu_tiles" + _SFX[self.dt])
+            self.fn.restype = C.c_double
+        else:
+            self.fn = getattr(_lib("oracle", None), "or_swift_cpu_tiles" + _SFX[self.dt])
+            self.fn.restype = None
+
+    def run(self, t0, t1, with_reside=False):
+        """Adds the product of tiles [t0, t1) (and the reside part) into self.C; returns
+        (seconds, nonzeros processed)."""
+        import time
+        a = time.perf_counter()
+        self.fn(C.byref(self.s), int(t0), int(t1), int(with_reside), self.M, self.K, self.N,
+                _p(self.sortB, _CT[self.dt]), _p(self.C, _CT[self.dt]))
+        sec = time.perf_counter() - a
+        nnz = (t1 - t0) * 32 + (int(self.s.reside_nnz) if with_reside else 0)
+        return sec, nnz

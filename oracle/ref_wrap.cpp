@@ -218,4 +218,25 @@ double REFN(ref_swift_cpu)(const or_slide_t *m, int M, int K, int N, const ref_t
   return (double)t;
 }
 
+// Swift_cpu unchanged, run on a view of tiles [t0, t1) (and the reside part if
+// with_reside): the tile arrays of the view start at tile t0 while slot indices stay
+// absolute, which is how Swift_cpu indexes them (src/Swift_cpu.h:31-50).  Used to time
+// bounded samples of a large workload.  Returns wall ms (steady clock).
+double REFN(ref_swift_cpu_tiles)(const or_slide_t *m, int t0, int t1, int with_reside, int M,
+                                 int K, int N, const ref_t *sortB, ref_t *C) {
+  slide_matrix s;
+  import_slide(m, &s);
+  s.tilenum = t1 - t0;
+  s.tile_ptr = m->tile_ptr + t0;
+  s.tile_len = m->tile_len + t0;
+  s.tile_colidx = m->tile_colidx + t0;
+  if (!with_reside) s.reside_col = 0;
+  ref_t t = 0;
+  timeval a, b;
+  gettimeofday(&a, nullptr);
+  Swift_cpu(t, &s, 0, M, K, N, const_cast<ref_t *>(sortB), C);
+  gettimeofday(&b, nullptr);
+  return (b.tv_sec - a.tv_sec) * 1000.0 + (b.tv_usec - a.tv_usec) / 1000.0;
+}
+
 }  // extern "C"

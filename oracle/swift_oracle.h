@@ -56,6 +56,8 @@ extern "C" {
   int or_row_idx_sort##SFX(or_slide##SFX *m, float *blockratio);                               \
   void or_swift_cpu##SFX(const or_slide##SFX *m, int M, int K, int N, const VAL_T *sortB,      \
                          VAL_T *C);                                                            \
+  void or_swift_cpu_tiles##SFX(const or_slide##SFX *m, int t0, int t1, int with_reside, int M,  \
+                               int K, int N, const VAL_T *sortB, VAL_T *C);                    \
   void or_slide_free##SFX(or_slide##SFX *m);
 
 OR_DECLARE(float, _f32)

@@ -302,6 +302,25 @@ void FN(or_swift_cpu)(const SLIDE *m, int M, int K, int N, const VAL_T *sortB, V
   }
 }
 
+/* The same product restricted to tiles [t0, t1) (plus the reside part if with_reside), for
+ * timing bounded samples of large workloads. */
+void FN(or_swift_cpu_tiles)(const SLIDE *m, int t0, int t1, int with_reside, int M, int K,
+                            int N, const VAL_T *sortB, VAL_T *C) {
+  SLIDE v = *m;
+  (void)M;
+  for (int t = t0; t < t1; ++t)
+    for (int l = 0; l < OR_TILE; ++l) {
+      long j = (long)t * OR_TILE + l;
+      int col = m->tile_colidx[t] + l, row = m->sortrowidx[j];
+      VAL_T w = m->sortval[j];
+      for (int n = 0; n < N; ++n) C[(size_t)row * N + n] += w * sortB[(size_t)col * N + n];
+    }
+  if (with_reside) {
+    v.tilenum = 0;
+    FN(or_swift_cpu)(&v, M, K, N, sortB, C);
+  }
+}
+
 void FN(or_slide_free)(SLIDE *m) {
   void *ps[] = {m->tile_ptr, m->tile_len, m->tile_colidx, m->tile_tall, m->sortrowidx,
                 m->sortval, m->reside_cscptr, m->reside_cscrowidx, m->reside_val,

@@ -29,7 +29,9 @@ size_t plan_device_bytes(const Plan &p) {
   for (const DevBuf *b : bufs) s += b->bytes;
   for (const RowLayout *L : {&p.fwd, &p.bwd}) {
     const DevBuf *lb[] = {&L->piece_row, &L->piece_idx, &L->long_first, &L->long_count,
-                          &L->long_of_row, &L->counters, &L->scratch};
+                          &L->long_of_row, &L->counters, &L->scratch, &L->task_row,
+                          &L->head_split, &L->tail_split, &L->split_row, &L->split_first,
+                          &L->split_last, &L->split_cnt, &L->mscratch, &L->task_hdr, &L->eidx};
     for (const DevBuf *b : lb) s += b->bytes;
   }
   return s;
@@ -58,6 +60,13 @@ static size_t dtype_size(swift_dtype d) {
     case SWIFT_F16: return 2;
   }
   return 0;
+}
+
+MergeOpts merge_opts_for(Plan &p, int N, swift_dtype dt) {
+  std::lock_guard<std::mutex> g(p.mu);
+  if (p.merge_override) return p.merge_opts;
+  auto it = p.tuned_merge.find({N, (int)dt});
+  return it != p.tuned_merge.end() ? it->second : p.merge_opts;
 }
 
 swift_status ensure_bwd(Plan &p, cudaStream_t st) {
@@ -263,7 +272,7 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
   if (engine == SWIFT_ENGINE_ROWWISE) {
     if (!row_ok) return SWIFT_ERR_UNSUPPORTED;
     if (p.M == 0) return SWIFT_OK;
-    return run_rowwise(p, p.fwd, d, st);
+    return run_merge(p, p.fwd, d, merge_opts_for(p, N, dtype), st);
   }
   if (engine == SWIFT_ENGINE_TILED) return run_tiled(p, d, 0, st);
   return SWIFT_ERR_INVALID_ARG;
@@ -281,7 +290,7 @@ swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dt
   if (p.K == 0 || N == 0) return SWIFT_OK;
   DenseArgs d;
   d.N = N; d.dtype = dtype; d.B = Y; d.ldb = ldy; d.C = X; d.ldc = ldx;
-  return run_rowwise(p, p.bwd, d, st);
+  return run_merge(p, p.bwd, d, MergeOpts{}, st);
 }
 
 swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const void *U,
@@ -324,7 +333,7 @@ swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_d
     SW_TRY(ensure_bwd(p, st));
     DenseArgs d;
     d.N = N; d.dtype = dtype; d.B = dY; d.ldb = lddy; d.C = dX; d.ldc = lddx;
-    SW_TRY(run_rowwise(p, p.bwd, d, st));
+    SW_TRY(run_merge(p, p.bwd, d, MergeOpts{}, st));
   }
   return SWIFT_OK;
 }
@@ -345,35 +354,90 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  struct Cand {
+    swift_engine eng;
+    MergeOpts mo;
+  };
+  std::vector<Cand> cands;
+  if (dtype != SWIFT_BF16 && dtype != SWIFT_F16) cands.push_back({SWIFT_ENGINE_TILED, MergeOpts{}});
+  if (p.has_csr) {
+    // task size (the work-balance grain) x (loads in flight, vector bytes, kernel variant)
+    const int shapes[][3] = {{4, 16, 1}, {8, 16, 1}, {4, 32, 1}, {4, 16, 2}, {4, 32, 2}};
+    for (int U : {128, 256, 512, 1024})
+      for (const auto &sh : shapes) {
+        MergeOpts mo;
+        mo.U = U;
+        mo.unroll = sh[0];
+        mo.vbytes = sh[1];
+        mo.kernel = sh[2];
+        cands.push_back({SWIFT_ENGINE_ROWWISE, mo});
+      }
+  }
+  const bool saved_override = p.merge_override;
+  const MergeOpts saved_opts = p.merge_opts;
   double best = 1e300;
-  swift_engine win = SWIFT_ENGINE_TILED;
-  const swift_engine cands[2] = {SWIFT_ENGINE_TILED, SWIFT_ENGINE_ROWWISE};
-  for (swift_engine eng : cands) {
-    if (eng == SWIFT_ENGINE_ROWWISE && !p.has_csr) continue;
-    if (eng == SWIFT_ENGINE_TILED && (dtype == SWIFT_BF16 || dtype == SWIFT_F16)) continue;
+  Cand win{SWIFT_ENGINE_TILED, MergeOpts{}};
+  for (const Cand &c : cands) {
+    p.merge_override = true;
+    p.merge_opts = c.mo;
     swift_status rc = SWIFT_OK;
     for (int w = 0; w < 2 && rc == SWIFT_OK; ++w)
-      rc = swift_spmm(plan, eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
+      rc = swift_spmm(plan, c.eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
     if (rc != SWIFT_OK) continue;
     const int reps = 5;
     cudaEventRecord(e0, st);
     for (int r = 0; r < reps; ++r)
-      swift_spmm(plan, eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
+      swift_spmm(plan, c.eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
     cudaEventRecord(e1, st);
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    if (ms / reps < best) { best = ms / reps; win = eng; }
+    if (ms / reps < best) { best = ms / reps; win = c; }
   }
+  p.merge_override = saved_override;
+  p.merge_opts = saved_opts;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (best >= 1e300) return SWIFT_ERR_UNSUPPORTED;
   {
     std::lock_guard<std::mutex> g(p.mu);
-    p.tuned[{N, (int)dtype}] = win;
+    p.tuned[{N, (int)dtype}] = win.eng;
+    if (win.eng == SWIFT_ENGINE_ROWWISE) p.tuned_merge[{N, (int)dtype}] = win.mo;
   }
   if (best_ms) *best_ms = best;
-  if (best_engine) *best_engine = win;
+  if (best_engine) *best_engine = win.eng;
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_set_rowwise_params(swift_plan *plan, int task_size, int loads_in_flight,
+                                           int vector_bytes, int kernel) {
+  if (!plan || task_size < 0 || kernel < 0 || kernel > 3) return SWIFT_ERR_INVALID_ARG;
+  if (vector_bytes != 0 && vector_bytes != 4 && vector_bytes != 16 && vector_bytes != 32)
+    return SWIFT_ERR_INVALID_ARG;
+  Plan &p = plan->p;
+  std::lock_guard<std::mutex> g(p.mu);
+  if (task_size == 0) {
+    p.merge_override = false;
+    p.merge_opts = MergeOpts{};
+    return SWIFT_OK;
+  }
+  p.merge_override = true;
+  p.merge_opts.U = task_size;
+  p.merge_opts.unroll = loads_in_flight > 0 ? loads_in_flight : 4;
+  p.merge_opts.vbytes = vector_bytes;
+  p.merge_opts.kernel = kernel;
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_get_rowwise_params(swift_plan *plan, int N, swift_dtype dtype,
+                                           int *task_size, int *loads_in_flight,
+                                           int *vector_bytes, int *kernel) {
+  if (!plan) return SWIFT_ERR_INVALID_ARG;
+  MergeOpts o = merge_opts_for(plan->p, N, dtype);
+  if (task_size) *task_size = o.U;
+  if (loads_in_flight) *loads_in_flight = o.unroll;
+  if (vector_bytes) *vector_bytes = o.vbytes;
+  if (kernel) *kernel = o.kernel;
   return SWIFT_OK;
 }
 

@@ -122,6 +122,23 @@ struct RowLayout {
   DevBuf scratch;        // partial sums, grown on demand: pieces * N * 8 bytes
   size_t scratch_bytes = 0;
   bool built = false;
+  // merge-path tasks (spmm_merge.cu): U positions of the merged nonzero/row-end sequence each
+  int merge_U = 0, ntasks = 0, nsplit = 0;
+  bool merge_built = false;
+  DevBuf task_row;                    // [ntasks+1] row holding each task's first position
+  DevBuf head_split, tail_split;      // [ntasks] split-row id of the task's first / last row or -1
+  DevBuf task_hdr;                    // [ntasks] int4 packing of the three arrays above
+  DevBuf eidx;                        // [nnz] gather indices, bit 31 set on each row's first
+  DevBuf split_row, split_first, split_last, split_cnt;  // [nsplit]
+  DevBuf mscratch;                    // [2*ntasks][N] partial rows
+};
+
+// Parameters of the merge-path row engine (autotuned per (N, dtype); overridable).
+struct MergeOpts {
+  int U = 512;      // merged positions per task
+  int unroll = 4;   // B-row loads in flight per lane and batch (4, 8 or 16)
+  int vbytes = 0;   // vector bytes per lane: 0 = widest the operands allow, 32, 16 or 4
+  int kernel = 0;   // 0 choose, 1 lean walk, 2 flagged-index walk, 3 general walk
 };
 
 struct Plan {
@@ -168,6 +185,9 @@ struct Plan {
   int long_row_split = 128;
   // autotuned choice per (N, dtype)
   std::map<std::pair<int, int>, swift_engine> tuned;
+  std::map<std::pair<int, int>, MergeOpts> tuned_merge;
+  bool merge_override = false;
+  MergeOpts merge_opts;  // used when set explicitly, and as the default otherwise
   std::mutex mu;  // guards lazily built layouts and scratch growth
 };
 
@@ -216,6 +236,9 @@ struct DenseArgs {
 // variant 1 = reside per column without balance blocks (Swift_gpu1's kernel)
 swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cudaStream_t st);
 swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &a, cudaStream_t st);
+swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpts &o,
+                       cudaStream_t st);
+swift_status build_merge_tasks(RowLayout &L, int U, cudaStream_t st);
 swift_status run_f64_reference(const Plan &p, int N, const double *B, int64_t ldb, double *C,
                                int64_t ldc, cudaStream_t st);
 swift_status run_sddmm(Plan &p, int N, swift_dtype dt, const void *U, int64_t ldu,

@@ -1,0 +1,682 @@
+// spmm_merge.cu -- row-ordered SpMM with merge-path work balance.
+//
+// The merged sequence of a CSR operand interleaves its nonzeros with one end marker per row
+// (row r occupies positions ptr[r]+r .. ptr[r+1]+r, the last being its end marker).  A task
+// is a fixed slice of U positions; a sub-warp walks its slice, keeping the current C row in
+// registers across nonzeros and storing it when it passes the row's end marker, so it never
+// waits on a row's metadata before issuing the next row's B loads, empty rows cost one
+// store, and power-law rows need no special casing.  A row whose positions straddle task
+// boundaries is "split": each task touching it stores its partial row to scratch and counts
+// its arrival; the last task to arrive adds the partials in task order and writes C, so the
+// result does not depend on scheduling.
+//
+// Memory-level parallelism: each lane keeps UNR independent B-row vectors in flight per batch
+// (16 for one vector per lane) and the next chunk of (index, value) pairs is fetched while
+// the current one is consumed.  Vectors are 32 bytes (sm_100 256-bit accesses) when the
+// operands allow, which halves the load instructions per byte against 16-byte vectors.
+#include "common.cuh"
+#include "vec.cuh"
+
+namespace swift {
+
+struct MergeArgs {
+  int rows, N, U, ntasks;
+  int64_t total;  // nnz + rows
+  const int *ptr, *idx;
+  const void *val;
+  const int *out_row;
+  const void *B;
+  int64_t ldb;
+  void *C;
+  int64_t ldc;
+  const int *task_row, *head_split, *tail_split;
+  const int *task_hdr;  // [ntasks] int4 (task_row[t], task_row[t+1], head_split, tail_split)
+  const int *split_row, *split_first, *split_last;
+  int *split_cnt;
+  void *scratch;  // [2 * ntasks][N] partial rows
+};
+
+namespace {
+
+// B vectors in flight per lane: 8 (16 when deep), capped so the batch holds at most 256 bytes
+// of accumulator-type values per lane (64 registers).
+constexpr int unroll_for(int VB, int VPL, bool deep, int acc_bytes) {
+  const int lim = 256 / (VB * VPL * acc_bytes) > 0 ? 256 / (VB * VPL * acc_bytes) : 1;
+  const int base = deep ? 16 : 8;
+  return base < lim ? base : lim;
+}
+
+template <class T, class ACC, int VB, int SG, int VPL>
+__device__ __forceinline__ void store_c(const MergeArgs &a, int row, int col0, int sl,
+                                        const ACC (&acc)[VPL][VB]) {
+  const int orow = a.out_row ? __ldg(a.out_row + row) : row;
+  T *dst = static_cast<T *>(a.C) + (int64_t)orow * a.ldc + col0 + sl * VB;
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+    if (col0 + v * SG * VB + sl * VB < a.N) vstore<T, ACC, VB>(dst + v * SG * VB, acc[v]);
+}
+
+template <class ACC, int VB, int SG, int VPL>
+__device__ __forceinline__ void store_partial(const MergeArgs &a, int slot, int col0, int sl,
+                                              const ACC (&acc)[VPL][VB]) {
+  ACC *dst = static_cast<ACC *>(a.scratch) + (int64_t)slot * a.N + col0 + sl * VB;
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+#pragma unroll
+    for (int e = 0; e < VB; ++e)
+      if (col0 + v * SG * VB + sl * VB + e < a.N) __stcg(dst + v * SG * VB + e, acc[v][e]);
+}
+
+// Counts this task's arrival for split row s; the last task adds the partials in task order.
+template <class T, class ACC, int VB, int SG, int VPL>
+__device__ __forceinline__ void arrive(const MergeArgs &a, int s, int sl, unsigned sgmask) {
+  __threadfence();
+  __syncwarp(sgmask);
+  int old = 0;
+  if (sl == 0) old = atomicAdd(a.split_cnt + s, 1);
+  old = __shfl_sync(sgmask, old, 0, SG);
+  const int ta = a.split_first[s], tb = a.split_last[s];
+  if (old != tb - ta) return;
+  __threadfence();
+  constexpr int CW = SG * VB * VPL;
+  const ACC *scr = static_cast<const ACC *>(a.scratch);
+  for (int col0 = 0; col0 < a.N; col0 += CW) {
+    ACC acc[VPL][VB];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v)
+#pragma unroll
+      for (int e = 0; e < VB; ++e) acc[v][e] = ACC(0);
+    for (int t = ta; t <= tb; ++t) {
+      const int slot = t == ta ? 2 * t + 1 : 2 * t;
+      const ACC *src = scr + (int64_t)slot * a.N + col0 + sl * VB;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v)
+#pragma unroll
+        for (int e = 0; e < VB; ++e)
+          if (col0 + v * SG * VB + sl * VB + e < a.N) acc[v][e] += __ldcg(src + v * SG * VB + e);
+    }
+    store_c<T, ACC, VB, SG, VPL>(a, a.split_row[s], col0, sl, acc);
+  }
+  __syncwarp(sgmask);
+  if (sl == 0) a.split_cnt[s] = 0;  // ready for the next product
+}
+
+template <class T, class TA, class ACC, int VB, int SG, int VPL, int UNR, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_spmm_kernel(const MergeArgs a) {
+  constexpr int G = 32 / SG;
+  constexpr int CW = SG * VB * VPL;
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  const int64_t d0 = (int64_t)t * a.U;
+  const int64_t d1 = d0 + a.U < a.total ? d0 + a.U : a.total;
+  const int r = __ldg(a.task_row + t), rn = __ldg(a.task_row + t + 1);
+  const int p = (int)(d0 - r), pn = (int)(d1 - rn);
+  const int hs = __ldg(a.head_split + t), ts = __ldg(a.tail_split + t);
+  const T *__restrict__ B = static_cast<const T *>(a.B);
+  const TA *__restrict__ val = static_cast<const TA *>(a.val);
+  for (int col0 = 0; col0 < a.N; col0 += CW) {
+    bool inb[VPL];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) inb[v] = col0 + v * SG * VB + sl * VB < a.N;
+    ACC acc[VPL][VB];
+#pragma unroll
+    for (int v = 0; v < VPL; ++v)
+#pragma unroll
+      for (int e = 0; e < VB; ++e) acc[v][e] = ACC(0);
+    int cur = r;
+    int rbase = cur;
+    int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+    int pe = __shfl_sync(sgmask, myend, 0, SG);
+    // stores row `cur` (or its head partial) and advances to the next row
+    auto finish_and_advance = [&]() {
+      if (cur == r && hs >= 0) store_partial<ACC, VB, SG, VPL>(a, 2 * t, col0, sl, acc);
+      else store_c<T, ACC, VB, SG, VPL>(a, cur, col0, sl, acc);
+#pragma unroll
+      for (int v = 0; v < VPL; ++v)
+#pragma unroll
+        for (int e = 0; e < VB; ++e) acc[v][e] = ACC(0);
+      ++cur;
+      if (cur - rbase >= SG) {
+        rbase = cur;
+        myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+      }
+      pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
+    };
+    // (index, value) pairs are fetched one chunk ahead of their use
+    int nxc = 0;
+    ACC nxv = ACC(0);
+    if (p + sl < pn) {
+      nxc = __ldcs(a.idx + p + sl);
+      nxv = (ACC)__ldcs(val + p + sl);
+    }
+    for (int q0 = p; q0 < pn; q0 += SG) {
+      const int m = min(SG, pn - q0);
+      const int myc = nxc;
+      const ACC myv = nxv;
+      if (q0 + SG + sl < pn) {
+        nxc = __ldcs(a.idx + q0 + SG + sl);
+        nxv = (ACC)__ldcs(val + q0 + SG + sl);
+      }
+      for (int k = 0; k < m; k += UNR) {
+        ACC b[UNR][VPL][VB];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const int c = __shfl_sync(sgmask, myc, (k + u) & (SG - 1), SG);
+          const bool ok = k + u < m;
+          const T *row = B + (int64_t)c * a.ldb + col0 + sl * VB;
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) {
+            if (ok && inb[v]) vload<T, ACC, VB>(row + v * SG * VB, b[u][v]);
+            else {
+#pragma unroll
+              for (int e = 0; e < VB; ++e) b[u][v][e] = ACC(0);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          if (k + u >= m) break;
+          const int q = q0 + k + u;
+          while (q == pe) finish_and_advance();
+          const ACC w = __shfl_sync(sgmask, myv, (k + u) & (SG - 1), SG);
+#pragma unroll
+          for (int v = 0; v < VPL; ++v)
+#pragma unroll
+            for (int e = 0; e < VB; ++e) acc[v][e] = fma(w, b[u][v][e], acc[v][e]);
+        }
+      }
+    }
+    while (cur < rn) finish_and_advance();
+    if (ts >= 0) store_partial<ACC, VB, SG, VPL>(a, (hs >= 0 && r == rn) ? 2 * t : 2 * t + 1, col0, sl, acc);
+  }
+  if (hs >= 0 && r < rn) arrive<T, ACC, VB, SG, VPL>(a, hs, sl, sgmask);
+  if (ts >= 0) arrive<T, ACC, VB, SG, VPL>(a, ts, sl, sgmask);
+}
+
+// Lean variant for the common case where one vector per lane spans the whole C row slice
+// (N <= SG * VB): the same walk with the least live state, so that up to 64 warps fit on an
+// SM -- for this gather pattern occupancy, not loads per warp, sets the throughput.
+template <class T, class TA, class ACC, int VB, int SG, int UNR, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a) {
+  constexpr int G = 32 / SG;
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
+  const int64_t d0 = (int64_t)t * a.U;
+  const int p = (int)(d0 - hdr.x);
+  const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
+  const bool inb = sl * VB < a.N;
+  ACC acc[VB];
+#pragma unroll
+  for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+  int cur = hdr.x, rbase = cur;
+  int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+  int pe = __shfl_sync(sgmask, myend, 0, SG);
+  auto finish_and_advance = [&]() {
+    if (cur == hdr.x && hdr.z >= 0) {
+      ACC *dst = static_cast<ACC *>(a.scratch) + (int64_t)(2 * t) * a.N + sl * VB;
+      if (inb) {
+#pragma unroll
+        for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+      }
+    } else if (inb) {
+      const int orow = a.out_row ? __ldg(a.out_row + cur) : cur;
+      vstore<T, ACC, VB>(static_cast<T *>(a.C) + (int64_t)orow * a.ldc + sl * VB, acc);
+    }
+#pragma unroll
+    for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+    ++cur;
+    if (cur - rbase >= SG) {
+      rbase = cur;
+      myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+    }
+    pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
+  };
+  const T *__restrict__ Bl = static_cast<const T *>(a.B) + sl * VB;
+  for (int q0 = p; q0 < pn; q0 += SG) {
+    const int m = min(SG, pn - q0);
+    int myc = 0;
+    ACC myv = ACC(0);
+    if (sl < m) {
+      myc = __ldcs(a.idx + q0 + sl);
+      myv = (ACC)__ldcs(static_cast<const TA *>(a.val) + q0 + sl);
+    }
+    for (int k = 0; k < m; k += UNR) {
+      ACC b[UNR][VB];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const int c = __shfl_sync(sgmask, myc, (k + u) & (SG - 1), SG);
+        if (k + u < m && inb) vload<T, ACC, VB>(Bl + (int64_t)c * a.ldb, b[u]);
+        else {
+#pragma unroll
+          for (int e = 0; e < VB; ++e) b[u][e] = ACC(0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        if (k + u >= m) break;
+        while (q0 + k + u == pe) finish_and_advance();
+        const ACC w = __shfl_sync(sgmask, myv, (k + u) & (SG - 1), SG);
+#pragma unroll
+        for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+      }
+    }
+  }
+  while (cur < hdr.y) finish_and_advance();
+  if (hdr.w >= 0 && inb) {
+    ACC *dst = static_cast<ACC *>(a.scratch) + (int64_t)((hdr.z >= 0 && hdr.x == hdr.y) ? 2 * t : 2 * t + 1) * a.N + sl * VB;
+#pragma unroll
+    for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+  }
+  if (hdr.z >= 0 && hdr.x < hdr.y) arrive<T, ACC, VB, SG, 1>(a, hdr.z, sl, sgmask);
+  if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1>(a, hdr.w, sl, sgmask);
+}
+
+// Streamlined walk: the execution copy of the gather indices carries bit 31 on the first
+// nonzero of every row, so the end-of-row bookkeeping is skipped unless a batch holds a row
+// start; (index, value) pairs of a 32-nonzero chunk are staged in shared memory and read back
+// with one broadcast load per nonzero; full chunks run fully unrolled.
+template <class T, class TA, class ACC, int VB, int SG, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
+  constexpr int G = 32 / SG;
+  constexpr int UNR = 4;
+  __shared__ int2 stage_all[8 * G][32];
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  int2 *stage = stage_all[(threadIdx.x >> 5) * G + sg];
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
+  const int64_t d0 = (int64_t)t * a.U;
+  const int p = (int)(d0 - hdr.x);
+  const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
+  const bool inb = sl * VB < a.N;
+  ACC acc[VB];
+#pragma unroll
+  for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+  int cur = hdr.x, rbase = cur;
+  int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+  int pe = __shfl_sync(sgmask, myend, 0, SG);
+  auto finish_and_advance = [&]() {
+    if (cur == hdr.x && hdr.z >= 0) {
+      ACC *dst = static_cast<ACC *>(a.scratch) + (int64_t)(2 * t) * a.N + sl * VB;
+      if (inb) {
+#pragma unroll
+        for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+      }
+    } else if (inb) {
+      const int orow = a.out_row ? __ldg(a.out_row + cur) : cur;
+      vstore<T, ACC, VB>(static_cast<T *>(a.C) + (int64_t)orow * a.ldc + sl * VB, acc);
+    }
+#pragma unroll
+    for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+    ++cur;
+    if (cur - rbase >= SG) {
+      rbase = cur;
+      myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+    }
+    pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
+  };
+  const char *Bl = reinterpret_cast<const char *>(static_cast<const T *>(a.B) + sl * VB);
+  const int64_t ldb_bytes = a.ldb * (int64_t)sizeof(T);
+  const TA *val = static_cast<const TA *>(a.val);
+  for (int q0 = p; q0 < pn; q0 += 32) {
+    const int m = min(32, pn - q0);
+    __syncwarp(sgmask);
+#pragma unroll
+    for (int j = sl; j < 32; j += SG) {
+      int2 e = make_int2(0, 0);
+      if (j < m) {
+        e.x = __ldcs(a.idx + q0 + j);
+        e.y = __float_as_int((float)__ldcs(val + q0 + j));
+      }
+      stage[j] = e;
+    }
+    __syncwarp(sgmask);
+    if (m == 32) {
+#pragma unroll 1
+      for (int k = 0; k < 32; k += UNR) {
+        ACC b[UNR][VB];
+        int flags = 0;
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const int c = stage[k + u].x;
+          flags |= c;
+          if (inb) vload<T, ACC, VB>(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes), b[u]);
+          else {
+#pragma unroll
+            for (int e = 0; e < VB; ++e) b[u][e] = ACC(0);
+          }
+        }
+        if (flags < 0) {
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) {
+            while (q0 + k + u == pe) finish_and_advance();
+            const ACC w = (ACC)__int_as_float(stage[k + u].y);
+#pragma unroll
+            for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) {
+            const ACC w = (ACC)__int_as_float(stage[k + u].y);
+#pragma unroll
+            for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+          }
+        }
+      }
+    } else {
+      for (int k = 0; k < m; ++k) {
+        const int c = stage[k].x;
+        ACC b[VB];
+        if (inb) vload<T, ACC, VB>(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes), b);
+        else {
+#pragma unroll
+          for (int e = 0; e < VB; ++e) b[e] = ACC(0);
+        }
+        while (q0 + k == pe) finish_and_advance();
+        const ACC w = (ACC)__int_as_float(stage[k].y);
+#pragma unroll
+        for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[e], acc[e]);
+      }
+    }
+  }
+  while (cur < hdr.y) finish_and_advance();
+  if (hdr.w >= 0 && inb) {
+    ACC *dst = static_cast<ACC *>(a.scratch) + (int64_t)((hdr.z >= 0 && hdr.x == hdr.y) ? 2 * t : 2 * t + 1) * a.N + sl * VB;
+#pragma unroll
+    for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+  }
+  if (hdr.z >= 0 && hdr.x < hdr.y) arrive<T, ACC, VB, SG, 1>(a, hdr.z, sl, sgmask);
+  if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1>(a, hdr.w, sl, sgmask);
+}
+
+// Execution copy of the gather indices with bit 31 on the first nonzero of every row.
+__global__ void row_start_set_kernel(const int *__restrict__ ptr, int rows, int *__restrict__ eidx) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x)
+    if (ptr[r + 1] > ptr[r]) eidx[ptr[r]] |= (int)0x80000000u;
+}
+
+// ------------------------------------------------------------------ plan-time task build
+// Packs (task_row[t], task_row[t+1], head_split[t], tail_split[t]) for the lean kernel.
+__global__ void task_hdr_kernel(const int *__restrict__ task_row, const int *__restrict__ hs,
+                                const int *__restrict__ ts, int ntasks, int4 *__restrict__ hdr) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks;
+       t += (int64_t)gridDim.x * blockDim.x)
+    hdr[t] = make_int4(task_row[t], task_row[t + 1], hs[t], ts[t]);
+}
+
+// task_row[t] = smallest row whose span reaches position t*U (rows for t = ntasks).
+__global__ void task_row_kernel(const int *__restrict__ ptr, int rows, int64_t total, int U,
+                                int ntasks, int *__restrict__ task_row) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= ntasks;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = t * (int64_t)U < total ? t * (int64_t)U : total;
+    int lo = 0, hi = rows;  // answer in [0, rows]
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((int64_t)__ldg(ptr + mid + 1) + mid >= d) hi = mid; else lo = mid + 1;
+    }
+    task_row[t] = (t == ntasks) ? rows : lo;
+  }
+}
+
+__global__ void split_flag_kernel(const int *__restrict__ ptr, int rows, int U, int *__restrict__ flag) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t first = (int64_t)ptr[r] + r, last = (int64_t)ptr[r + 1] + r;
+    flag[r] = (first / U) != (last / U);
+  }
+}
+
+__global__ void split_fill_kernel(const int *__restrict__ ptr, int rows, int U,
+                                  const int *__restrict__ pos, int *__restrict__ split_row,
+                                  int *__restrict__ split_first, int *__restrict__ split_last,
+                                  int *__restrict__ head_split, int *__restrict__ tail_split) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t first = (int64_t)ptr[r] + r, last = (int64_t)ptr[r + 1] + r;
+    const int ta = (int)(first / U), tb = (int)(last / U);
+    if (ta == tb) continue;
+    const int s = pos[r];
+    split_row[s] = (int)r;
+    split_first[s] = ta;
+    split_last[s] = tb;
+    tail_split[ta] = s;
+    head_split[tb] = s;
+    for (int t = ta + 1; t < tb; ++t) { head_split[t] = s; tail_split[t] = s; }
+  }
+}
+
+int grid_n(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+}  // namespace
+
+swift_status build_merge_tasks(RowLayout &L, int U, cudaStream_t st) {
+  if (L.merge_U == U && L.merge_built) return SWIFT_OK;
+  const int rows = L.rows;
+  const int64_t total = (int64_t)L.nnz + rows;
+  const int64_t nt = (total + U - 1) / U;
+  if (nt >= INT32_MAX / 2) return SWIFT_ERR_OVERFLOW;
+  L.ntasks = (int)nt;
+  SW_TRY(L.task_row.alloc(sizeof(int) * ((size_t)nt + 1)));
+  SW_TRY(L.head_split.alloc(sizeof(int) * (size_t)std::max<int64_t>(nt, 1)));
+  SW_TRY(L.tail_split.alloc(sizeof(int) * (size_t)std::max<int64_t>(nt, 1)));
+  SW_CHECK_CUDA(cudaMemsetAsync(L.head_split.p, 0xff, L.head_split.bytes, st));
+  SW_CHECK_CUDA(cudaMemsetAsync(L.tail_split.p, 0xff, L.tail_split.bytes, st));
+  task_row_kernel<<<grid_n(nt + 1), 256, 0, st>>>(L.ptr, rows, total, U, (int)nt, L.task_row.as<int>());
+  SW_CHECK_LAUNCH();
+  TmpBuf flag;
+  SW_TRY(flag.alloc(sizeof(int) * ((size_t)rows + 1), st));
+  if (rows > 0) split_flag_kernel<<<grid_n(rows), 256, 0, st>>>(L.ptr, rows, U, flag.as<int>());
+  SW_CHECK_LAUNCH();
+  SW_TRY(scan_exclusive_i32(flag.as<int>(), flag.as<int>(), rows, st));
+  int ns = 0;
+  SW_CHECK_CUDA(cudaMemcpyAsync(&ns, flag.as<int>() + rows, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  L.nsplit = ns;
+  SW_TRY(L.split_row.alloc(sizeof(int) * (size_t)ns));
+  SW_TRY(L.split_first.alloc(sizeof(int) * (size_t)ns));
+  SW_TRY(L.split_last.alloc(sizeof(int) * (size_t)ns));
+  SW_TRY(L.split_cnt.alloc(sizeof(int) * (size_t)ns));
+  SW_CHECK_CUDA(cudaMemsetAsync(L.split_cnt.p, 0, L.split_cnt.bytes, st));
+  if (rows > 0)
+    split_fill_kernel<<<grid_n(rows), 256, 0, st>>>(L.ptr, rows, U, flag.as<int>(), L.split_row.as<int>(),
+                                                    L.split_first.as<int>(), L.split_last.as<int>(),
+                                                    L.head_split.as<int>(), L.tail_split.as<int>());
+  SW_CHECK_LAUNCH();
+  SW_TRY(L.task_hdr.alloc(sizeof(int4) * (size_t)std::max<int64_t>(nt, 1)));
+  if (nt > 0)
+    task_hdr_kernel<<<grid_n(nt), 256, 0, st>>>(L.task_row.as<int>(), L.head_split.as<int>(),
+                                                L.tail_split.as<int>(), (int)nt, L.task_hdr.as<int4>());
+  SW_CHECK_LAUNCH();
+  if (!L.eidx.p) {
+    SW_TRY(L.eidx.alloc(sizeof(int) * (size_t)L.nnz));
+    if (L.nnz > 0) {
+      SW_CHECK_CUDA(cudaMemcpyAsync(L.eidx.p, L.idx, sizeof(int) * (size_t)L.nnz, cudaMemcpyDeviceToDevice, st));
+      if (rows > 0) row_start_set_kernel<<<grid_n(rows), 256, 0, st>>>(L.ptr, rows, L.eidx.as<int>());
+      SW_CHECK_LAUNCH();
+    }
+  }
+  L.merge_U = U;
+  L.merge_built = true;
+  return SWIFT_OK;
+}
+
+namespace {
+
+template <class T, class TA, class ACC, int VB, int SG, int VPL, int UNR, int MINB = 4>
+swift_status launch_merge(const MergeArgs &a, cudaStream_t st) {
+  constexpr int G = 32 / SG;
+  const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
+  if (warps == 0) return SWIFT_OK;
+  merge_spmm_kernel<T, TA, ACC, VB, SG, VPL, UNR, MINB><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+// Lean-kernel shape: at most `want` loads in flight, no more than 256 bytes of batch per lane;
+// blocks per SM from an estimate of 28 registers of walk state plus batch and accumulators.
+constexpr int lean_unr(int VB, int AB, int want) {
+  const int lim = 256 / (VB * AB) > 0 ? 256 / (VB * AB) : 1;
+  return want < lim ? want : lim;
+}
+constexpr int lean_minb(int VB, int AB, int UNR) {
+  const int regs = 28 + (UNR + 1) * VB * AB / 4;
+  const int b = 65536 / (256 * regs);
+  return b < 1 ? 1 : (b > 8 ? 8 : b);
+}
+
+template <class T, class TA, class ACC, int VB, int SG, int MINB>
+swift_status launch_flag(MergeArgs a, const int *eidx, cudaStream_t st) {
+  constexpr int G = 32 / SG;
+  const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
+  if (warps == 0) return SWIFT_OK;
+  a.idx = eidx;
+  merge_flag_kernel<T, TA, ACC, VB, SG, MINB><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+template <class T, class TA, class ACC, int VB, int SG, int UNR, int MINB>
+swift_status launch_lean(const MergeArgs &a, cudaStream_t st) {
+  constexpr int G = 32 / SG;
+  const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
+  if (warps == 0) return SWIFT_OK;
+  merge_lean_kernel<T, TA, ACC, VB, SG, UNR, MINB><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+// unr = loads in flight per lane and batch: 4 or 8 (lean kernel when one vector per lane
+// covers N), 16 ("deep", general kernel), else the shape's default
+template <class T, class TA, class ACC>
+swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, int kernel,
+                         const int *eidx, cudaStream_t st) {
+  constexpr int V = VecWidth<T>::value;
+  constexpr int W = WideWidth<T>::value;
+  constexpr int AB = (int)sizeof(ACC);
+  // flagged-index kernel (FP32-valued plans): 4 loads in flight
+#define SW_MCASE_FLAG(VB_, SG_)                                                                 \
+  if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_)                                   \
+    return launch_flag<T, TA, ACC, VB_, SG_, lean_minb(VB_, AB, 4)>(a, eidx, st);
+  if (sizeof(TA) == 4 && (kernel == 2 || (kernel == 0 && unr <= 4))) {
+    SW_MCASE_FLAG(W, 2)
+    SW_MCASE_FLAG(W, 4)
+    SW_MCASE_FLAG(W, 8)
+    SW_MCASE_FLAG(W, 16)
+    SW_MCASE_FLAG(W, 32)
+    SW_MCASE_FLAG(V, 2)
+    SW_MCASE_FLAG(V, 4)
+    SW_MCASE_FLAG(V, 8)
+    SW_MCASE_FLAG(V, 16)
+    SW_MCASE_FLAG(V, 32)
+    SW_MCASE_FLAG(1, 32)
+  }
+#undef SW_MCASE_FLAG
+#define SW_MCASE(VB_, SG_, VPL_)                                                              \
+  if (VB == VB_ && SG == SG_ && VPL == VPL_)                                                    \
+    return launch_merge<T, TA, ACC, VB_, SG_, VPL_, unroll_for(VB_, VPL_, false, AB)>(a, st);
+#define SW_MCASE_DEEP(VB_, SG_)                                                                 \
+  if (VB == VB_ && SG == SG_ && VPL == 1 && unr >= 16 &&                                        \
+      unroll_for(VB_, 1, true, AB) > unroll_for(VB_, 1, false, AB))                             \
+    return launch_merge<T, TA, ACC, VB_, SG_, 1, unroll_for(VB_, 1, true, AB), 2>(a, st);
+  // lean kernel: one vector per lane; 4 (or 8) loads in flight, with the blocks per SM the
+  // register estimate of the walk allows
+#define SW_MCASE_LEAN(VB_, SG_)                                                                 \
+  if (kernel != 3 && VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_ && unr <= 4)        \
+    return launch_lean<T, TA, ACC, VB_, SG_, lean_unr(VB_, AB, 4), lean_minb(VB_, AB, lean_unr(VB_, AB, 4))>(a, st); \
+  if (kernel != 3 && VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_ && unr <= 8)        \
+    return launch_lean<T, TA, ACC, VB_, SG_, lean_unr(VB_, AB, 8), lean_minb(VB_, AB, lean_unr(VB_, AB, 8))>(a, st);
+  SW_MCASE_LEAN(W, 2)
+  SW_MCASE_LEAN(W, 4)
+  SW_MCASE_LEAN(W, 8)
+  SW_MCASE_LEAN(W, 16)
+  SW_MCASE_LEAN(W, 32)
+  SW_MCASE_LEAN(V, 2)
+  SW_MCASE_LEAN(V, 4)
+  SW_MCASE_LEAN(V, 8)
+  SW_MCASE_LEAN(V, 16)
+  SW_MCASE_LEAN(V, 32)
+  SW_MCASE_LEAN(1, 32)
+  SW_MCASE(W, 2, 1)
+  SW_MCASE(W, 4, 1)
+  SW_MCASE(W, 8, 1)
+  SW_MCASE(W, 16, 1)
+  SW_MCASE(W, 32, 1)
+  SW_MCASE(W, 32, 2)
+  SW_MCASE_DEEP(V, 16)
+  SW_MCASE_DEEP(V, 32)
+  SW_MCASE(V, 2, 1)
+  SW_MCASE(V, 4, 1)
+  SW_MCASE(V, 8, 1)
+  SW_MCASE(V, 16, 1)
+  SW_MCASE(V, 32, 1)
+  SW_MCASE(V, 32, 2)
+  SW_MCASE(V, 32, 4)
+  SW_MCASE(1, 32, 1)
+#undef SW_MCASE
+#undef SW_MCASE_DEEP
+#undef SW_MCASE_LEAN
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpts &o,
+                       cudaStream_t st) {
+  {
+    std::lock_guard<std::mutex> g(p.mu);
+    SW_TRY(build_merge_tasks(L, o.U > 0 ? o.U : 256, st));
+    const size_t acc = (p.val_type == SWIFT_F64) ? 8 : 4;
+    const size_t need = (size_t)2 * L.ntasks * (size_t)d.N * acc;
+    if (need > L.mscratch.bytes) SW_TRY(L.mscratch.alloc(need));
+  }
+  MergeArgs a{};
+  a.rows = L.rows; a.N = d.N; a.U = L.merge_U; a.ntasks = L.ntasks;
+  a.total = (int64_t)L.nnz + L.rows;
+  a.ptr = L.ptr; a.idx = L.idx; a.val = L.val; a.out_row = L.out_row;
+  a.B = d.B; a.ldb = d.ldb; a.C = d.C; a.ldc = d.ldc;
+  a.task_row = L.task_row.as<int>(); a.head_split = L.head_split.as<int>(); a.tail_split = L.tail_split.as<int>();
+  a.task_hdr = L.task_hdr.as<int>();
+  a.split_row = L.split_row.as<int>(); a.split_first = L.split_first.as<int>();
+  a.split_last = L.split_last.as<int>(); a.split_cnt = L.split_cnt.as<int>();
+  a.scratch = L.mscratch.p;
+  const size_t esz = d.dtype == SWIFT_F64 ? 8 : (d.dtype == SWIFT_F32 ? 4 : 2);
+  auto aligned = [&](int bytes) {
+    return ((uintptr_t)d.B % bytes == 0) && ((uintptr_t)d.C % bytes == 0) &&
+           ((d.ldb * (int64_t)esz) % bytes == 0) && ((d.ldc * (int64_t)esz) % bytes == 0) &&
+           (d.N % (int)(bytes / esz) == 0);
+  };
+  // vector width: 32 bytes when aligned and at most two vectors per lane cover the row slice,
+  // else 16 bytes, else scalar
+  int VB = 1;
+  if (o.vbytes != 16 && o.vbytes != 4 && aligned(32) && d.N / (int)(32 / esz) <= 64) VB = (int)(32 / esz);
+  else if (o.vbytes != 4 && aligned(16)) VB = (int)(16 / esz);
+  const int lanes = (d.N + VB - 1) / VB;
+  int SG = 32, VPL = 1;
+  if (VB > 1) {
+    SG = 2;
+    while (SG < lanes && SG < 32) SG <<= 1;
+    if (lanes > 32) VPL = lanes > 64 ? 4 : 2;
+  }
+#define SW_MDISPATCH(T, TA, ACC) return merge_shape<T, TA, ACC>(a, VB, SG, VPL, o.unroll, o.kernel, L.eidx.as<int>(), st);
+  if (p.val_type == SWIFT_F64) {
+    if (d.dtype != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+    SW_MDISPATCH(double, double, double)
+  }
+  switch (d.dtype) {
+    case SWIFT_F32: SW_MDISPATCH(float, float, float)
+    case SWIFT_BF16: SW_MDISPATCH(__nv_bfloat16, float, float)
+    case SWIFT_F16: SW_MDISPATCH(__half, float, float)
+    default: return SWIFT_ERR_UNSUPPORTED;
+  }
+#undef SW_MDISPATCH
+}
+
+}  // namespace swift

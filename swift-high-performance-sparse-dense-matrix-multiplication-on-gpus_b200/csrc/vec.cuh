@@ -8,6 +8,21 @@
 namespace swift {
 
 template <class T> struct VecWidth { static constexpr int value = 16 / sizeof(T); };
+// 32-byte vectors (sm_100 256-bit global loads / stores)
+template <class T> struct WideWidth { static constexpr int value = 32 / sizeof(T); };
+
+__device__ __forceinline__ void ld_nc_v8(const void *p, unsigned (&r)[8]) {
+  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "l"(p));
+}
+
+__device__ __forceinline__ void st_cs_v8(void *p, const unsigned (&r)[8]) {
+  asm volatile("st.global.cs.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
 
 template <class ACC, class T> __device__ __forceinline__ ACC to_acc(T x) { return (ACC)x; }
 template <> __device__ __forceinline__ float to_acc<float, __nv_bfloat16>(__nv_bfloat16 x) { return __bfloat162float(x); }
@@ -22,6 +37,12 @@ template <class T, class ACC, int VB>
 __device__ __forceinline__ void vload(const T *__restrict__ p, ACC (&o)[VB]) {
   if constexpr (VB == 1) {
     o[0] = to_acc<ACC>(__ldg(p));
+  } else if constexpr (sizeof(T) * VB == 32) {
+    unsigned r[8];
+    ld_nc_v8(p, r);
+    const T *h = reinterpret_cast<const T *>(r);
+#pragma unroll
+    for (int i = 0; i < VB; ++i) o[i] = to_acc<ACC>(h[i]);
   } else if constexpr (sizeof(T) == 4 && VB == 4) {
     float4 f = __ldg(reinterpret_cast<const float4 *>(p));
     o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
@@ -43,6 +64,12 @@ __device__ __forceinline__ void vstore(T *__restrict__ p, const ACC (&a)[VB]) {
   if constexpr (VB == 1) {
     if constexpr (sizeof(T) >= 4) __stcs(p, from_acc<T>(a[0]));
     else *p = from_acc<T>(a[0]);
+  } else if constexpr (sizeof(T) * VB == 32) {
+    unsigned r[8];
+    T *h = reinterpret_cast<T *>(r);
+#pragma unroll
+    for (int i = 0; i < VB; ++i) h[i] = from_acc<T>(a[i]);
+    st_cs_v8(p, r);
   } else if constexpr (sizeof(T) == 4 && VB == 4) {
     __stcs(reinterpret_cast<float4 *>(p), make_float4(a[0], a[1], a[2], a[3]));
   } else if constexpr (sizeof(T) == 8 && VB == 2) {

@@ -247,6 +247,21 @@ class Plan:
                    "swift_spmm_f64_reference")
         return out
 
+    def set_rowwise_params(self, task_size=0, loads_in_flight=0, vector_bytes=0, kernel=0):
+        """Overrides the row engine's task size, loads in flight per lane, vector width and
+        kernel variant (0 choose, 1 lean, 2 flagged indices, 3 general); task_size=0 returns to
+        the tuned / default parameters."""
+        capi.check(capi.lib().swift_plan_set_rowwise_params(self._h, int(task_size), int(loads_in_flight),
+                                                            int(vector_bytes), int(kernel)),
+                   "swift_plan_set_rowwise_params")
+
+    def rowwise_params(self, N, dtype):
+        v = [C.c_int(0) for _ in range(4)]
+        capi.check(capi.lib().swift_plan_get_rowwise_params(self._h, int(N), _dtype_code(dtype),
+                                                            *[C.byref(x) for x in v]),
+                   "swift_plan_get_rowwise_params")
+        return dict(zip(("task_size", "loads_in_flight", "vector_bytes", "kernel"), (x.value for x in v)))
+
     def autotune(self, B, C_out, stream=None):
         ms = C.c_double(0)
         eng = C.c_int(0)

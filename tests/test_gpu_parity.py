@@ -136,6 +136,27 @@ def test_long_row_split_is_deterministic(split):
     pl.close()
 
 
+@pytest.mark.parametrize("U", [7, 32, 128, 256, 1024])
+@pytest.mark.parametrize("unr,vb,kern", [(4, 0, 1), (8, 0, 1), (4, 16, 2), (4, 32, 2), (16, 16, 3),
+                                         (8, 32, 3), (4, 4, 0)])
+@pytest.mark.parametrize("N", [8, 33, 128, 300, 512])
+def test_row_engine_parameters(U, unr, vb, kern, N):
+    """Every task size, load depth, vector width and kernel variant gives the same
+    (deterministic) product; rows split across tasks are combined in task order."""
+    M, K, rp, ci = cases.make("rmat12", 1)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    Bn = gen.dense_uniform(K, N, 2, np.float32)
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, Bn)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    pl.set_rowwise_params(U, unr, vb, kern)
+    B = tdev(Bn)
+    c1 = pl.spmm(B, engine="rowwise")
+    c2 = pl.spmm(B, engine="rowwise")
+    assert torch.equal(c1, c2)
+    assert relerr(c1.cpu().numpy(), ref) <= 1e-5
+    pl.close()
+
+
 @pytest.mark.parametrize("dt16", ["bf16", "f16"])
 def test_low_precision_operands(dt16):
     M, K, rp, ci = cases.make("rmat12", 0)
