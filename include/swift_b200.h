@@ -227,6 +227,29 @@ swift_status swift_spmm_f64_reference(const swift_plan *plan, int N, const doubl
                                       int64_t ldb, double *C, int64_t ldc,
                                       swift_stream_t stream);
 
+/* C = A * B for callers that cannot allocate device memory once running -- real-time or
+ * certified deployments that forbid device allocation after start-up, and hosts whose device
+ * memory belongs to another allocator (a framework's caching allocator, a fixed arena), where
+ * a stray cudaMalloc can fail or fragment that memory and synchronises the device.  No
+ * counterpart in the reference.
+ *
+ * Same result as swift_spmm with the ROWWISE engine on row-major B (K x N) and C (M x N), but
+ * it calls no cudaMalloc, cudaFree or allocating routine: the scratch of the long-row pieces
+ * lives in a fixed device array of SWIFT_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until the process exits.  The plan must already exist (creating it
+ * allocates).
+ * Limits: at most SWIFT_NOALLOC_MAX_LONG_ROWS long rows and pieces * N * 4 bytes (8 for FP64)
+ * of partial rows within the array minus 64 KiB; larger products return SWIFT_ERR_OVERFLOW
+ * (details in swift_last_error) -- a plan made with a larger long_row_split has fewer pieces.
+ * The first call on each device looks up the array's device address with that device
+ * current, so make it before any stream capture.  All calls share the array and it keeps the
+ * last call's contents (each call clears the counters it uses): calls that overlap on the GPU
+ * race, so serialise them. */
+#define SWIFT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+#define SWIFT_NOALLOC_MAX_LONG_ROWS 16384
+swift_status swift_spmm_noalloc(const swift_plan *plan, int N, swift_dtype dtype, const void *B,
+                                int64_t ldb, void *C, int64_t ldc, swift_stream_t stream);
+
 /* ------------------------------------------------------------------ tuning */
 /* Times the engines and their parameters on this plan for (N, dtype) with CUDA events and
  * stores the fastest as the plan's AUTO choice.  B and C are caller buffers of the right

@@ -79,10 +79,6 @@ swift_status ensure_bwd(Plan &p, cudaStream_t st) {
 
 using namespace swift;
 
-struct swift_plan {
-  Plan p;
-};
-
 extern "C" {
 
 const char *swift_status_string(swift_status s) {

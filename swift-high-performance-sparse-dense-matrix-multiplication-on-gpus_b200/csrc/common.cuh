@@ -258,4 +258,12 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+swift_status run_rowwise_external(Plan &p, RowLayout &L, const DenseArgs &d, void *scratch,
+                                  int *counters, cudaStream_t st);
+
 }  // namespace swift
+
+// The opaque handle of the C ABI.
+struct swift_plan {
+  swift::Plan p;
+};

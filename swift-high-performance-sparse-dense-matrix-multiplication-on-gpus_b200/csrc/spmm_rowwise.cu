@@ -362,6 +362,37 @@ static swift_status run_layout(Plan &p, RowLayout &L, int N, swift_dtype dt, con
 #undef SW_DISPATCH
 }
 
+// The row kernel with caller-provided scratch for the long-row partials and arrival counters
+// (pieces * N accumulator values, long_rows counters that must be zero on entry).  Used by
+// the entry point that allocates nothing (spmm_noalloc.cu).
+swift_status run_rowwise_external(Plan &p, RowLayout &L, const DenseArgs &d, void *scratch,
+                                  int *counters, cudaStream_t st) {
+  if (d.b_layout != SWIFT_ROW_MAJOR || d.c_layout != SWIFT_ROW_MAJOR || d.b_presorted)
+    return SWIFT_ERR_UNSUPPORTED;
+  RowKArgs a{};
+  a.rows = L.rows; a.N = d.N; a.split = L.split; a.pieces = L.pieces; a.all_short = 0;
+  a.rows_per_sg = 2;
+  a.ptr = L.ptr; a.idx = L.idx; a.val = L.val; a.out_row = L.out_row;
+  a.B = d.B; a.ldb = d.ldb; a.C = d.C; a.ldc = d.ldc;
+  a.long_of_row = L.long_of_row.as<int>(); a.piece_row = L.piece_row.as<int>();
+  a.piece_idx = L.piece_idx.as<int>(); a.long_first = L.long_first.as<int>();
+  a.long_count = L.long_count.as<int>();
+  a.counters = counters;
+  a.scratch = scratch;
+  const size_t esz = d.dtype == SWIFT_F64 ? 8 : (d.dtype == SWIFT_F32 ? 4 : 2);
+  const bool vec_ok = aligned16(d.B, d.ldb, esz) && aligned16(d.C, d.ldc, esz) && (d.N % (int)(16 / esz) == 0);
+  if (p.val_type == SWIFT_F64) {
+    if (d.dtype != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
+    return launch_shape<double, double, double, true, false>(a, pick_shape<double>(d.N, vec_ok), st);
+  }
+  switch (d.dtype) {
+    case SWIFT_F32: return launch_shape<float, float, float, true, false>(a, pick_shape<float>(d.N, vec_ok), st);
+    case SWIFT_BF16: return launch_shape<__nv_bfloat16, float, float, true, false>(a, pick_shape<__nv_bfloat16>(d.N, vec_ok), st);
+    case SWIFT_F16: return launch_shape<__half, float, float, true, false>(a, pick_shape<__half>(d.N, vec_ok), st);
+    default: return SWIFT_ERR_UNSUPPORTED;
+  }
+}
+
 swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &d, cudaStream_t st) {
   if (d.b_layout != SWIFT_ROW_MAJOR || d.c_layout != SWIFT_ROW_MAJOR || d.b_presorted)
     return SWIFT_ERR_UNSUPPORTED;
