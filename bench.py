@@ -37,6 +37,8 @@ WORKLOADS = {
     "rmat20_n32_f32": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f32"),
     "rmat20_n128_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=128, dtype="f64"),
     "rmat20_n32_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f64"),
+    # half-size case for full ncu captures (B and C still exceed L2)
+    "rmat19_n128_f32": dict(kind="rmat", scale=19, edges=8 << 20, N=128, dtype="f32"),
     # precision workload: R-MAT scale 19 avg degree 32 merged with a 64-wide band, 16-bit B/C
     "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
     "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),
@@ -158,17 +160,21 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_from_profile(kernel, workload):
-    """dram bytes per launch from the committed ncu summary of this kernel and workload."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
-    try:
+def profile_summary(workload):
+    """The committed ncu summary of this workload's top kernel: `key: value` lines of
+    profiles/<kernel>_<workload>.txt (kernel, dram_bytes_per_launch, ...), or {}."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"*_{workload}.txt"))):
+        d = {}
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+                if ":" in line and not line.startswith(" "):
+                    k, v = line.split(":", 1)
+                    d[k.strip()] = v.strip()
+        if "dram_bytes_per_launch" in d and "kernel" in d:
+            d["file"] = os.path.relpath(path, ROOT)
+            return d
+    return {}
 
 
 class _StdoutToStderr:
@@ -283,8 +289,9 @@ def run_ours(args):
     alg_bytes = nnz * (vsz + 4) + K * N * esz + M * N * esz
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
-    kernel = "rowwise_kernel" if engine == "rowwise" else "tiled_rowmajor_kernel"
-    traffic = traffic_from_profile(kernel, args.workload)
+    prof = profile_summary(args.workload)
+    kernel = prof.get("kernel", "merge engine" if engine == "rowwise" else "tiled_rowmajor_kernel")
+    traffic = float(prof["dram_bytes_per_launch"].split()[0]) if prof else None
 
     # the Swift tiled engine on the same inputs (reported beside the chosen engine)
     tiled = None
@@ -363,6 +370,7 @@ def run_ours(args):
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} ({'MEASURED_PEAKS.json hbm_gbs' if peak_kind == 'measured' else 'pool fallback'})",
                      "kernel": kernel, "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic_source": prof.get("file"),
                      "frac_of_8TBs_nominal": achieved / 8000.0},
         "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": int(Bh.numel() * Bh.element_size()),
                 "d2h_bytes_per_step": int(Ch.numel() * Ch.element_size()), "steps": args.e2e_steps,

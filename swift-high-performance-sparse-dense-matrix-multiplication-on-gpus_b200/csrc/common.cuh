@@ -212,6 +212,15 @@ swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *
 swift_status build_tiles(Plan &p, cudaStream_t st);
 // Tiled-engine work items from tile_colidx (also used for plans made from a slide_matrix).
 swift_status build_items(Plan &p, cudaStream_t st);
+// Balance blocks from p.reside_ptr (device) and its host copy.
+swift_status build_balance(Plan &p, const int *h_reside_ptr, cudaStream_t st);
+// Tile formats (and fmt_count) from p.sortrowidx.
+swift_status classify_tiles(Plan &p, cudaStream_t st);
+swift_status stable_column_order(const int *d_cnt, int K, int *d_perm, int *d_invperm,
+                                 int *d_sortnnz, int *max_count, cudaStream_t st);
+swift_status csr_to_csc_device(const int *d_rowptr, const int *d_colidx, const void *d_val,
+                               bool f64, int M, int K, int nnz, int *d_colptr, int *d_rowidx,
+                               void *d_cscval, int *d_cnt, cudaStream_t st);
 swift_status build_row_layout(Plan &p, RowLayout &L, bool transpose, cudaStream_t st);
 // Segment arrays of block_catgory on device (countrow[tilenum+1], segmentoffset[segsum+1],
 // sortrowindex[32*tilenum]); segsum returned on host.

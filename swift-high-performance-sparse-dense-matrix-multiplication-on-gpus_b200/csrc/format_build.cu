@@ -381,6 +381,29 @@ __global__ void long_fill_kernel(const int *__restrict__ ptr, int rows, int spli
   }
 }
 
+// src/block_catgory.h:11-72 on an existing tile array: one warp per tile.
+__global__ void classify_kernel(const int *__restrict__ rows, int T, int *__restrict__ fmt_out,
+                                int *__restrict__ fmt_count) {
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int l = threadIdx.x & 31;
+  int f0 = 0, f1 = 0, f2 = 0;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < T; t += warps) {
+    const int r = rows[(int64_t)t * kTile + l];
+    const int up = __shfl_up_sync(0xffffffffu, r, 1);
+    const int changes = __popc(__ballot_sync(0xffffffffu, l > 0 && up != r));
+    const int fmt = changes == 0 ? 0 : (changes < 16 ? 2 : 1);
+    if (l == 0) {
+      fmt_out[t] = fmt;
+      f0 += fmt == 0; f1 += fmt == 1; f2 += fmt == 2;
+    }
+  }
+  if (l == 0) {
+    if (f0) atomicAdd(&fmt_count[0], f0);
+    if (f1) atomicAdd(&fmt_count[1], f1);
+    if (f2) atomicAdd(&fmt_count[2], f2);
+  }
+}
+
 __global__ void item_flags_kernel(const int *__restrict__ colidx, int T, int *__restrict__ flag) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < T;
        t += (int64_t)gridDim.x * blockDim.x)
@@ -427,6 +450,103 @@ swift_status build_items(Plan &p, cudaStream_t st) {
   SW_TRY(p.item_tile.alloc(sizeof(int) * ((size_t)n + 1)));
   item_fill_kernel<<<grid_for(T + 1), 256, 0, st>>>(p.tile_colidx.as<int>(), T, flags.as<int>(),
                                                      p.item_tile.as<int>());
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+// Balance blocks of the reside part (src/balance.h:1-69): the block count comes from the
+// host-visible reside pointer, the arrays are filled on the device from p.reside_ptr.
+swift_status build_balance(Plan &p, const int *h_reside_ptr, cudaStream_t st) {
+  int nb = 0;
+  for (int q = 0; q < p.reside_col; ++q) {
+    int len = h_reside_ptr[q + 1] - h_reside_ptr[q];
+    nb += len <= kTile ? 1 : (len + kTile - 1) / kTile;
+  }
+  p.numblk = nb;
+  SW_TRY(p.colorblk.alloc(sizeof(unsigned) * (size_t)nb));
+  SW_TRY(p.blkstart.alloc(sizeof(int) * (size_t)nb));
+  SW_TRY(p.blkstop.alloc(sizeof(int) * (size_t)nb));
+  SW_TRY(p.blkptr.alloc(sizeof(int) * (size_t)nb));
+  if (nb > 0) {
+    SW_CHECK_CUDA(cudaMemsetAsync(p.blkstart.p, 0, sizeof(int) * nb, st));
+    SW_CHECK_CUDA(cudaMemsetAsync(p.blkstop.p, 0, sizeof(int) * nb, st));
+    SW_CHECK_CUDA(cudaMemsetAsync(p.blkptr.p, 0, sizeof(int) * nb, st));
+    balance_kernel<<<1, 32, 0, st>>>(p.reside_col, p.reside_ptr.as<int>(), p.colorblk.as<unsigned>(),
+                                     p.blkstart.as<int>(), p.blkstop.as<int>(), p.blkptr.as<int>());
+    SW_CHECK_LAUNCH();
+  }
+  return SWIFT_OK;
+}
+
+// Tile formats from p.sortrowidx alone (block_catgory on a format built elsewhere).
+swift_status classify_tiles(Plan &p, cudaStream_t st) {
+  SW_TRY(p.tile_format.alloc(sizeof(int) * ((size_t)p.tilenum + 3)));
+  TmpBuf fmt;
+  SW_TRY(fmt.alloc(sizeof(int) * 4, st));
+  SW_CHECK_CUDA(cudaMemsetAsync(fmt.p, 0, sizeof(int) * 4, st));
+  if (p.tilenum > 0)
+    classify_kernel<<<grid_for((int64_t)p.tilenum * 32, 256, 148 * 32), 256, 0, st>>>(
+        p.sortrowidx.as<int>(), p.tilenum, p.tile_format.as<int>(), fmt.as<int>());
+  SW_CHECK_LAUNCH();
+  int hf[4];
+  SW_CHECK_CUDA(cudaMemcpyAsync(hf, fmt.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 3; ++i) p.fmt_count[i] = hf[i];
+  return SWIFT_OK;
+}
+
+// Stable ascending order of K columns by count (ties by index): perm, invperm, sorted counts.
+swift_status stable_column_order(const int *d_cnt, int K, int *d_perm, int *d_invperm,
+                                 int *d_sortnnz, int *max_count, cudaStream_t st) {
+  if (K == 0) return SWIFT_OK;
+  TmpBuf k0, v0, k1, v1, mx;
+  SW_TRY(k0.alloc(sizeof(uint32_t) * (size_t)K, st));
+  SW_TRY(v0.alloc(sizeof(uint32_t) * (size_t)K, st));
+  SW_TRY(k1.alloc(sizeof(uint32_t) * (size_t)K, st));
+  SW_TRY(v1.alloc(sizeof(uint32_t) * (size_t)K, st));
+  SW_TRY(mx.alloc(sizeof(int) * 4, st));
+  SW_TRY(reduce_max_i32(d_cnt, K, mx.as<int>(), st));
+  int hmax = 0;
+  SW_CHECK_CUDA(cudaMemcpyAsync(&hmax, mx.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (max_count) *max_count = hmax;
+  copy_i32_to_u32<<<grid_for(K), 256, 0, st>>>(d_cnt, k0.as<uint32_t>(), K);
+  iota_kernel<<<grid_for(K), 256, 0, st>>>(v0.as<uint32_t>(), K);
+  SW_TRY(radix_sort_pairs(k0.as<uint32_t>(), v0.as<uint32_t>(), k1.as<uint32_t>(), v1.as<uint32_t>(),
+                          K, bitlen((uint32_t)hmax), st));
+  perm_finish_kernel<<<grid_for(K), 256, 0, st>>>(v1.as<uint32_t>(), d_cnt, K, d_perm, d_invperm, d_sortnnz);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+// CSR -> CSC on the device (src/gpu_csr2csc.h:51-157 semantics): counts, column pointer, and
+// entries in column order with rows ascending within a column.
+swift_status csr_to_csc_device(const int *d_rowptr, const int *d_colidx, const void *d_val,
+                               bool f64, int M, int K, int nnz, int *d_colptr, int *d_rowidx,
+                               void *d_cscval, int *d_cnt, cudaStream_t st) {
+  SW_CHECK_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * (size_t)std::max(K, 1), st));
+  if (nnz) col_count_kernel<<<grid_for(nnz), 256, 0, st>>>(d_colidx, nnz, d_cnt);
+  SW_CHECK_LAUNCH();
+  SW_TRY(scan_exclusive_i32(d_cnt, d_colptr, K, st));
+  if (nnz == 0) return SWIFT_OK;
+  TmpBuf k0, v0, k1, v1, pos;
+  SW_TRY(k0.alloc(sizeof(uint32_t) * (size_t)nnz, st));
+  SW_TRY(v0.alloc(sizeof(uint32_t) * (size_t)nnz, st));
+  SW_TRY(k1.alloc(sizeof(uint32_t) * (size_t)nnz, st));
+  SW_TRY(v1.alloc(sizeof(uint32_t) * (size_t)nnz, st));
+  SW_TRY(pos.alloc(sizeof(int) * (size_t)nnz, st));
+  copy_i32_to_u32<<<grid_for(nnz), 256, 0, st>>>(d_colidx, k0.as<uint32_t>(), nnz);
+  iota_kernel<<<grid_for(nnz), 256, 0, st>>>(v0.as<uint32_t>(), nnz);
+  SW_TRY(radix_sort_pairs(k0.as<uint32_t>(), v0.as<uint32_t>(), k1.as<uint32_t>(), v1.as<uint32_t>(),
+                          nnz, bitlen((uint32_t)(K - 1)), st));
+  if (f64)
+    sorted_csc_gather_kernel<double><<<grid_for(nnz), 256, 0, st>>>(
+        v1.as<uint32_t>(), d_rowptr, M, static_cast<const double *>(d_val), nnz, d_rowidx,
+        static_cast<double *>(d_cscval), pos.as<int>());
+  else
+    sorted_csc_gather_kernel<float><<<grid_for(nnz), 256, 0, st>>>(
+        v1.as<uint32_t>(), d_rowptr, M, static_cast<const float *>(d_val), nnz, d_rowidx,
+        static_cast<float *>(d_cscval), pos.as<int>());
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
 }
@@ -516,25 +636,7 @@ swift_status build_tiles(Plan &p, cudaStream_t st) {
           p.reside_ptr.as<int>(), p.reside_row.as<int>(), p.reside_val.as<float>());
     SW_CHECK_LAUNCH();
   }
-  // balance: block count from the (host-visible) reside lengths, arrays filled on device
-  int nb = 0;
-  for (int q = 0; q < p.reside_col; ++q) {
-    int len = rptr[q + 1] - rptr[q];
-    nb += len <= kTile ? 1 : (len + kTile - 1) / kTile;
-  }
-  p.numblk = nb;
-  SW_TRY(p.colorblk.alloc(sizeof(unsigned) * (size_t)nb));
-  SW_TRY(p.blkstart.alloc(sizeof(int) * (size_t)nb));
-  SW_TRY(p.blkstop.alloc(sizeof(int) * (size_t)nb));
-  SW_TRY(p.blkptr.alloc(sizeof(int) * (size_t)nb));
-  if (nb > 0) {
-    SW_CHECK_CUDA(cudaMemsetAsync(p.blkstart.p, 0, sizeof(int) * nb, st));
-    SW_CHECK_CUDA(cudaMemsetAsync(p.blkstop.p, 0, sizeof(int) * nb, st));
-    SW_CHECK_CUDA(cudaMemsetAsync(p.blkptr.p, 0, sizeof(int) * nb, st));
-    balance_kernel<<<1, 32, 0, st>>>(p.reside_col, p.reside_ptr.as<int>(), p.colorblk.as<unsigned>(),
-                                     p.blkstart.as<int>(), p.blkstop.as<int>(), p.blkptr.as<int>());
-    SW_CHECK_LAUNCH();
-  }
+  SW_TRY(build_balance(p, rptr, st));
   SW_TRY(build_items(p, st));
   int hf[4];
   SW_CHECK_CUDA(cudaMemcpyAsync(hf, fmt.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
@@ -562,9 +664,8 @@ swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *
   }
   p.has_csr = true;
 
-  TmpBuf err, maxbuf;
+  TmpBuf err;
   SW_TRY(err.alloc(sizeof(int) * 4, st));
-  SW_TRY(maxbuf.alloc(sizeof(int) * 4, st));
   SW_CHECK_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int) * 4, st));
   validate_csr_kernel<int><<<grid_for(std::max(M, nnz)), 256, 0, st>>>(p.rowptr.as<int>(), p.colidx.as<int>(),
                                                                        M, K, nnz, err.as<int>());
@@ -604,22 +705,15 @@ swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *
       SW_CHECK_CUDA(cudaStreamSynchronize(st));
       if (herr) return SWIFT_ERR_BAD_PERM;
       if (K) copy_i32_to_u32<<<grid_for(K), 256, 0, st>>>(p.perm.as<int>(), v1.as<uint32_t>(), K);
-    } else if (K) {
+      if (K) perm_finish_kernel<<<grid_for(K), 256, 0, st>>>(v1.as<uint32_t>(), p.cnt.as<int>(), K,
+                                                             p.perm.as<int>(), p.invperm.as<int>(),
+                                                             p.sortnnz.as<int>());
+      SW_CHECK_LAUNCH();
+    } else {
       // stable ascending sort of (count, column): thrust::sort_by_key order
-      SW_TRY(reduce_max_i32(p.cnt.as<int>(), K, maxbuf.as<int>(), st));
-      int hmax = 0;
-      SW_CHECK_CUDA(cudaMemcpyAsync(&hmax, maxbuf.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-      SW_CHECK_CUDA(cudaStreamSynchronize(st));
-      p.max_col = hmax;
-      copy_i32_to_u32<<<grid_for(K), 256, 0, st>>>(p.cnt.as<int>(), k0.as<uint32_t>(), K);
-      iota_kernel<<<grid_for(K), 256, 0, st>>>(v0.as<uint32_t>(), K);
-      SW_TRY(radix_sort_pairs(k0.as<uint32_t>(), v0.as<uint32_t>(), k1.as<uint32_t>(),
-                              v1.as<uint32_t>(), K, bitlen((uint32_t)hmax), st));
+      SW_TRY(stable_column_order(p.cnt.as<int>(), K, p.perm.as<int>(), p.invperm.as<int>(),
+                                 p.sortnnz.as<int>(), &p.max_col, st));
     }
-    if (K) perm_finish_kernel<<<grid_for(K), 256, 0, st>>>(v1.as<uint32_t>(), p.cnt.as<int>(), K,
-                                                           p.perm.as<int>(), p.invperm.as<int>(),
-                                                           p.sortnnz.as<int>());
-    SW_CHECK_LAUNCH();
   }
   SW_TRY(scan_exclusive_i32(p.sortnnz.as<int>(), p.sptr.as<int>(), K, st));
 

@@ -62,6 +62,54 @@ def _slide(vt):
 swift_slide_matrix_f32 = _slide(C.c_float)
 swift_slide_matrix_f64 = _slide(C.c_double)
 
+# array name -> (length as a function of the struct, numpy dtype; None = the value type)
+_SLIDE_LEN = {
+    "tile_ptr": (lambda s: s.tilenum + 1, "i4"), "tile_len": (lambda s: s.tilenum, "i4"),
+    "tile_colidx": (lambda s: s.tilenum, "i4"), "tile_tall": (lambda s: s.tilenum, "i4"),
+    "tile_format": (lambda s: s.tilenum, "i4"), "sortrowidx": (lambda s: s.regular_nnz, "i4"),
+    "sortval": (lambda s: s.regular_nnz, None), "countrow": (lambda s: s.tilenum + 1, "i4"),
+    "segmentoffset": (lambda s: s.segsum + 1, "i4"), "sortrowindex": (lambda s: s.regular_nnz, "i4"),
+    "val_position": (lambda s: s.regular_nnz, "i4"), "val_offset": (lambda s: s.regular_nnz, "i4"),
+    "reside_cscptr": (lambda s: s.reside_col + 1, "i4"), "reside_cscrowidx": (lambda s: s.reside_nnz, "i4"),
+    "reside_val": (lambda s: s.reside_nnz, None), "colorblk": (lambda s: s.numblk, "u4"),
+    "blkstart": (lambda s: s.numblk, "i4"), "blkstop": (lambda s: s.numblk, "i4"),
+    "blkptr": (lambda s: s.numblk, "i4"),
+}
+_SLIDE_INTS = ("tilenum", "regular_nnz", "reside_col", "reside_nnz", "numblk", "segsum")
+
+
+def slide_arrays(s, vdt, with_row_sort=True) -> dict:
+    """numpy copies of the arrays a slide_matrix struct holds (NULL pointers are skipped)."""
+    import numpy as np
+    out = {k: int(getattr(s, k)) for k in _SLIDE_INTS}
+    for name, (n_of, dt) in _SLIDE_LEN.items():
+        if not with_row_sort and name in ("val_position", "val_offset"):
+            continue
+        ptr, n = getattr(s, name), n_of(s)
+        if not ptr:
+            continue
+        out[name] = (np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt or vdt, copy=True)
+                     if n > 0 else np.zeros(0, dt or vdt))
+    return out
+
+
+def slide_from_arrays(d: dict, vdt):
+    """A slide_matrix struct pointing at numpy arrays of `d`; returns (struct, keep-alive list)."""
+    import numpy as np
+    S = swift_slide_matrix_f64 if np.dtype(vdt) == np.float64 else swift_slide_matrix_f32
+    s, keep = S(), []
+    for k in _SLIDE_INTS:
+        setattr(s, k, int(d.get(k, 0)))
+    for name, (_, dt) in _SLIDE_LEN.items():
+        if name not in d:
+            continue
+        a = np.ascontiguousarray(d[name], dtype=dt or vdt)
+        if a.size == 0:
+            a = np.zeros(1, dt or vdt)
+        keep.append(a)
+        setattr(s, name, a.ctypes.data_as(type(getattr(s, name))))
+    return s, keep
+
 _lib = None
 
 # (name, restype, argtypes)
@@ -95,6 +143,22 @@ _SIGS = [
     ("swift_batch_run", C.c_int, [_P, _P]),
     ("swift_batch_run_graph", C.c_int, [_P, _P]),
 ]
+# reference-convention functions (host buffers), one per value type
+_FP = C.POINTER(C.c_float)
+for _sfx, _S in (("f32", swift_slide_matrix_f32), ("f64", swift_slide_matrix_f64)):
+    _SP = C.POINTER(_S)
+    _SIGS += [
+        (f"swift_ref_csr_to_csc_{_sfx}", C.c_int, [_FP, C.c_int, C.c_int, C.c_int] + [_P] * 7),
+        (f"swift_ref_col_sort_{_sfx}", C.c_int, [_FP, C.c_int, C.c_int, C.c_int] + [_P] * 9),
+        (f"swift_ref_formattransation_{_sfx}", C.c_int,
+         [_FP, _SP, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+        (f"swift_ref_formatTransform_{_sfx}", C.c_int,
+         [_FP, _SP, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+        (f"swift_ref_block_catgory_{_sfx}", C.c_int, [_SP, C.POINTER(C.c_double)]),
+        (f"swift_ref_balance_{_sfx}", C.c_int, [_SP, C.c_int, C.c_int, C.c_int, _P, _P]),
+        (f"swift_ref_row_idx_sort_{_sfx}", C.c_int, [_SP, C.c_int, C.c_int, C.c_int, _FP]),
+        (f"swift_ref_spmm_{_sfx}", C.c_int, [C.c_int, _SP, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _FP]),
+    ]
 
 
 def lib():

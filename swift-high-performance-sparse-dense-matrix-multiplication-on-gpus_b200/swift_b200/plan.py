@@ -135,35 +135,8 @@ class Plan:
         br = C.c_float(0)
         fn = capi.lib().swift_plan_export_f64 if f64 else capi.lib().swift_plan_export_f32
         capi.check(fn(self._h, C.byref(s), int(with_row_sort), C.byref(br)), "swift_plan_export")
-        vdt = np.float64 if f64 else np.float32
-
-        def arr(ptr, n, dt):
-            if n <= 0 or not ptr:
-                return np.zeros(0, dt)
-            return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt, copy=True)
-
-        T, R, RC, RN, NB = s.tilenum, s.regular_nnz, s.reside_col, s.reside_nnz, s.numblk
-        out = dict(tilenum=T, regular_nnz=R, reside_col=RC, reside_nnz=RN, numblk=NB, segsum=s.segsum)
-        out["tile_ptr"] = arr(s.tile_ptr, T + 1, np.int32)
-        out["tile_len"] = arr(s.tile_len, T, np.int32)
-        out["tile_colidx"] = arr(s.tile_colidx, T, np.int32)
-        out["tile_tall"] = arr(s.tile_tall, T, np.int32)
-        out["tile_format"] = arr(s.tile_format, T, np.int32)
-        out["sortrowidx"] = arr(s.sortrowidx, R, np.int32)
-        out["sortval"] = arr(s.sortval, R, vdt)
-        out["countrow"] = arr(s.countrow, T + 1, np.int32)
-        out["segmentoffset"] = arr(s.segmentoffset, s.segsum + 1, np.int32)
-        out["sortrowindex"] = arr(s.sortrowindex, R, np.int32)
-        out["reside_cscptr"] = arr(s.reside_cscptr, RC + 1, np.int32)
-        out["reside_cscrowidx"] = arr(s.reside_cscrowidx, RN, np.int32)
-        out["reside_val"] = arr(s.reside_val, RN, vdt)
-        out["colorblk"] = arr(s.colorblk, NB, np.uint32)
-        out["blkstart"] = arr(s.blkstart, NB, np.int32)
-        out["blkstop"] = arr(s.blkstop, NB, np.int32)
-        out["blkptr"] = arr(s.blkptr, NB, np.int32)
+        out = capi.slide_arrays(s, np.float64 if f64 else np.float32, with_row_sort)
         if with_row_sort:
-            out["val_position"] = arr(s.val_position, R, np.int32)
-            out["val_offset"] = arr(s.val_offset, R, np.int32)
             out["blockratio"] = np.float32(br.value)
         (capi.lib().swift_slide_free_f64 if f64 else capi.lib().swift_slide_free_f32)(C.byref(s))
         return out
