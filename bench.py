@@ -39,6 +39,8 @@ WORKLOADS = {
     "rmat20_n32_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f64"),
     # half-size case for full ncu captures (B and C still exceed L2)
     "rmat19_n128_f32": dict(kind="rmat", scale=19, edges=8 << 20, N=128, dtype="f32"),
+    # half-size case for full ncu captures (B and C still exceed L2)
+    "rmat19_n128_f32": dict(kind="rmat", scale=19, edges=8 << 20, N=128, dtype="f32"),
     # precision workload: R-MAT scale 19 avg degree 32 merged with a 64-wide band, 16-bit B/C
     "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
     "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),

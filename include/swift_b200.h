@@ -273,20 +273,33 @@ swift_status swift_plan_get_rowwise_params(swift_plan *plan, int N, swift_dtype 
                                            int *vector_bytes, int *kernel);
 
 /* ------------------------------------------------------------------ batches */
-/* Many independent products C_i = A_i * B_i (row-major, F32) in one persistent launch. */
+/* Many independent products C_i = A_i * B_i (FP32 plans, FP32 row-major B_i and C_i) in one
+ * persistent launch: every SM runs resident blocks whose warps stride over the merge-path
+ * tasks of all members.  Each member keeps its own task layout, split-row counters and
+ * scratch, so a batch shares no mutable state with its plans' own products.  The plans must
+ * outlive the batch.  One batch must not run on two streams at once. */
 typedef struct swift_batch swift_batch;
 swift_status swift_batch_create(swift_plan *const *plans, int count, swift_stream_t stream,
                                 swift_batch **out);
+/* Synchronises the device before freeing the members' buffers. */
 swift_status swift_batch_destroy(swift_batch *batch);
-/* Ns[i], B[i], ldb[i], C[i], ldc[i] per matrix (device pointers, row-major).  Capturable in
- * a CUDA graph once set: swift_batch_set_operands uploads the operand table, then
- * swift_batch_run only launches. */
+/* Ns[i], B[i], ldb[i], C[i], ldc[i] per member (device pointers, row-major).  N_i <= 128 with
+ * 16-byte aligned operands (N_i % 4 == 0), or N_i <= 32 otherwise.  Builds the members' task
+ * layouts (first call, or after autotuning) and uploads the launch table; synchronises
+ * `stream`.  A graph captured by swift_batch_run_graph reads the table when it replays, so it
+ * stays valid when operands are set again. */
 swift_status swift_batch_set_operands(swift_batch *batch, const int *Ns, const void *const *B,
                                       const int64_t *ldb, void *const *C, const int64_t *ldc,
                                       swift_stream_t stream);
+/* One launch; writes every row of every C_i. */
 swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream);
-/* Captures swift_batch_run into a CUDA graph and replays it (graph kept by the batch). */
+/* Captures swift_batch_run into a CUDA graph on the first call (on a private stream) and
+ * replays it on `stream`. */
 swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream);
+/* Times the batch with tasks of 256, 512 and 1024 merged positions and keeps the fastest
+ * (operands must be set; each C_i is overwritten with its product). */
+swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, double *best_ms,
+                                  int *best_task_size);
 
 /* ------------------------------------------------------------------ reference calling convention */
 /* The reference's preprocessing and kernels with its host-buffer convention: inputs and

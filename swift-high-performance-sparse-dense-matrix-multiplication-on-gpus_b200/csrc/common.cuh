@@ -270,6 +270,15 @@ __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 swift_status run_rowwise_external(Plan &p, RowLayout &L, const DenseArgs &d, void *scratch,
                                   int *counters, cudaStream_t st);
 
+// Batched products (spmm_merge.cu): one launch record per member, a persistent grid.
+size_t merge_args_size();
+swift_status merge_batch_member(const Plan &p, RowLayout &L, int U, int N, const void *B, int64_t ldb,
+                                void *C, int64_t ldc, void *args_out, int *shape, int64_t *items,
+                                cudaStream_t st);
+swift_status merge_batch_grid(int device, int *grid);
+swift_status launch_merge_batch(const void *d_args, const int *d_shape, const int64_t *d_item_off,
+                                int count, int grid, cudaStream_t st);
+
 }  // namespace swift
 
 // The opaque handle of the C ABI.

@@ -1,0 +1,226 @@
+// spmm_batch.cu -- many independent products C_i = A_i * B_i in one persistent launch.
+//
+// Each member keeps its own merge-path task layout over its plan's CSR (so a batch never
+// shares task arrays, split counters or scratch with the plan's own products); the launch
+// records of all members live in one device table that the persistent kernel reads, so
+// setting new operands only rewrites the table and a captured CUDA graph stays valid.
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+struct swift_batch {
+  struct Operands {
+    std::vector<int> N;
+    std::vector<const void *> B;
+    std::vector<int64_t> ldb;
+    std::vector<void *> C;
+    std::vector<int64_t> ldc;
+  };
+  int device = 0;
+  int count = 0;
+  int U = 512;
+  int grid = 0;
+  std::vector<swift_plan *> plans;
+  std::vector<std::unique_ptr<swift::RowLayout>> layouts;
+  std::vector<unsigned char> h_args;
+  std::vector<int> h_shape;
+  std::vector<int64_t> h_off;
+  swift::DevBuf d_args, d_shape, d_off;
+  Operands ops;
+  bool ready = false;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~swift_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+using namespace swift;
+
+namespace {
+
+cudaStream_t to_stream(swift_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+swift_status on_device(const swift_batch *b) {
+  int dev = -1;
+  SW_CHECK_CUDA(cudaGetDevice(&dev));
+  if (dev != b->device) {
+    set_last_error("swift_batch", "the current device is not the batch's device");
+    return SWIFT_ERR_INVALID_ARG;
+  }
+  return SWIFT_OK;
+}
+
+// (Re)builds every member's launch record from the stored operands and uploads the table.
+swift_status build_table(swift_batch *b, cudaStream_t st) {
+  const size_t asz = merge_args_size();
+  int64_t off = 0;
+  for (int i = 0; i < b->count; ++i) {
+    b->h_off[i] = off;
+    int64_t items = 0;
+    SW_TRY(merge_batch_member(b->plans[i]->p, *b->layouts[i], b->U, b->ops.N[i], b->ops.B[i], b->ops.ldb[i],
+                              b->ops.C[i], b->ops.ldc[i], b->h_args.data() + asz * i, &b->h_shape[i], &items,
+                              st));
+    off += items;
+  }
+  b->h_off[b->count] = off;
+  if (b->count > 0) {
+    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_args.p, b->h_args.data(), asz * b->count, cudaMemcpyHostToDevice, st));
+    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_shape.p, b->h_shape.data(), sizeof(int) * b->count,
+                                  cudaMemcpyHostToDevice, st));
+  }
+  SW_CHECK_CUDA(cudaMemcpyAsync(b->d_off.p, b->h_off.data(), sizeof(int64_t) * (b->count + 1),
+                                cudaMemcpyHostToDevice, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));  // the host table may change after return
+  b->ready = true;
+  return SWIFT_OK;
+}
+
+swift_status launch(swift_batch *b, cudaStream_t st) {
+  return launch_merge_batch(b->d_args.p, b->d_shape.as<int>(), static_cast<const int64_t *>(b->d_off.p),
+                            b->count, b->grid, st);
+}
+
+swift_status check_ready(const swift_batch *b, const char *where) {
+  if (!b) return SWIFT_ERR_INVALID_ARG;
+  if (!b->ready) {
+    set_last_error(where, "operands not set");
+    return SWIFT_ERR_INVALID_ARG;
+  }
+  return on_device(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+swift_status swift_batch_create(swift_plan *const *plans, int count, swift_stream_t stream,
+                                swift_batch **out) {
+  (void)stream;
+  if (!out || count < 0 || (count > 0 && !plans)) return SWIFT_ERR_INVALID_ARG;
+  *out = nullptr;
+  int dev = 0;
+  SW_CHECK_CUDA(cudaGetDevice(&dev));
+  for (int i = 0; i < count; ++i) {
+    if (!plans[i]) return SWIFT_ERR_INVALID_ARG;
+    const Plan &p = plans[i]->p;
+    if (p.device != dev) {
+      set_last_error("swift_batch_create", "plans of one batch must live on the current device");
+      return SWIFT_ERR_INVALID_ARG;
+    }
+    if (p.val_type != SWIFT_F32 || !p.has_csr) {
+      set_last_error("swift_batch_create", "batches take FP32 plans built from CSR");
+      return SWIFT_ERR_UNSUPPORTED;
+    }
+  }
+  std::unique_ptr<swift_batch> b(new (std::nothrow) swift_batch());
+  if (!b) return SWIFT_ERR_ALLOC;
+  b->device = dev;
+  b->count = count;
+  b->plans.assign(plans, plans + count);
+  for (int i = 0; i < count; ++i) b->layouts.emplace_back(new RowLayout());
+  b->h_args.assign(merge_args_size() * (size_t)std::max(count, 1), 0);
+  b->h_shape.assign((size_t)std::max(count, 1), 0);
+  b->h_off.assign((size_t)count + 1, 0);
+  SW_TRY(b->d_args.alloc(b->h_args.size()));
+  SW_TRY(b->d_shape.alloc(sizeof(int) * b->h_shape.size()));
+  SW_TRY(b->d_off.alloc(sizeof(int64_t) * b->h_off.size()));
+  SW_TRY(merge_batch_grid(dev, &b->grid));
+  *out = b.release();
+  return SWIFT_OK;
+}
+
+swift_status swift_batch_destroy(swift_batch *batch) {
+  if (!batch) return SWIFT_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();  // members' buffers may still be in use by a launch in flight
+  delete batch;
+  return SWIFT_OK;
+}
+
+swift_status swift_batch_set_operands(swift_batch *batch, const int *Ns, const void *const *B,
+                                      const int64_t *ldb, void *const *C, const int64_t *ldc,
+                                      swift_stream_t stream) {
+  if (!batch) return SWIFT_ERR_INVALID_ARG;
+  const int n = batch->count;
+  if (n > 0 && (!Ns || !B || !ldb || !C || !ldc)) return SWIFT_ERR_INVALID_ARG;
+  SW_TRY(on_device(batch));
+  for (int i = 0; i < n; ++i) {
+    const Plan &p = batch->plans[i]->p;
+    if (Ns[i] < 0 || ldb[i] < Ns[i] || ldc[i] < Ns[i] || ldb[i] < 1 || ldc[i] < 1) return SWIFT_ERR_INVALID_ARG;
+    if (Ns[i] > 0 && ((p.K > 0 && !B[i]) || (p.M > 0 && !C[i]))) return SWIFT_ERR_INVALID_ARG;
+  }
+  batch->ready = false;
+  batch->ops.N.assign(Ns, Ns + n);
+  batch->ops.B.assign(B, B + n);
+  batch->ops.ldb.assign(ldb, ldb + n);
+  batch->ops.C.assign(C, C + n);
+  batch->ops.ldc.assign(ldc, ldc + n);
+  return build_table(batch, to_stream(stream));
+}
+
+swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream) {
+  SW_TRY(check_ready(batch, "swift_batch_run"));
+  return launch(batch, to_stream(stream));
+}
+
+swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream) {
+  SW_TRY(check_ready(batch, "swift_batch_run_graph"));
+  if (!batch->exec) {
+    // captured on a private stream (the legacy default stream cannot be captured)
+    if (!batch->cap) SW_CHECK_CUDA(cudaStreamCreateWithFlags(&batch->cap, cudaStreamNonBlocking));
+    SW_CHECK_CUDA(cudaStreamBeginCapture(batch->cap, cudaStreamCaptureModeThreadLocal));
+    const swift_status rc = launch(batch, batch->cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(batch->cap, &g);
+    if (rc != SWIFT_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    SW_CHECK_CUDA(ce);
+    batch->graph = g;
+    SW_CHECK_CUDA(cudaGraphInstantiate(&batch->exec, batch->graph, 0));
+  }
+  SW_CHECK_CUDA(cudaGraphLaunch(batch->exec, to_stream(stream)));
+  return SWIFT_OK;
+}
+
+swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, double *best_ms,
+                                  int *best_task_size) {
+  SW_TRY(check_ready(batch, "swift_batch_autotune"));
+  cudaStream_t st = to_stream(stream);
+  cudaEvent_t e0, e1;
+  SW_CHECK_CUDA(cudaEventCreate(&e0));
+  SW_CHECK_CUDA(cudaEventCreate(&e1));
+  double best = 1e300;
+  int bestU = batch->U;
+  swift_status rc = SWIFT_OK;
+  for (int U : {256, 512, 1024}) {
+    batch->U = U;
+    rc = build_table(batch, st);
+    for (int w = 0; w < 2 && rc == SWIFT_OK; ++w) rc = launch(batch, st);
+    if (rc != SWIFT_OK) break;
+    const int reps = 5;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && rc == SWIFT_OK; ++r) rc = launch(batch, st);
+    cudaEventRecord(e1, st);
+    if (rc != SWIFT_OK) break;
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms / reps < best) { best = ms / reps; bestU = U; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  batch->U = bestU;
+  if (rc == SWIFT_OK) rc = build_table(batch, st);
+  if (rc != SWIFT_OK) return rc;
+  if (best_ms) *best_ms = best;
+  if (best_task_size) *best_task_size = bestU;
+  return SWIFT_OK;
+}
+
+}  // extern "C"

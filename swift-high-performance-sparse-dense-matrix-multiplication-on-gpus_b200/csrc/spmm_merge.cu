@@ -14,6 +14,8 @@
 // (16 for one vector per lane) and the next chunk of (index, value) pairs is fetched while
 // the current one is consumed.  Vectors are 32 bytes (sm_100 256-bit accesses) when the
 // operands allow, which halves the load instructions per byte against 16-byte vectors.
+#include <cstring>
+
 #include "common.cuh"
 #include "vec.cuh"
 
@@ -280,16 +282,12 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
 // nonzero of every row, so the end-of-row bookkeeping is skipped unless a batch holds a row
 // start; (index, value) pairs of a 32-nonzero chunk are staged in shared memory and read back
 // with one broadcast load per nonzero; full chunks run fully unrolled.
-template <class T, class TA, class ACC, int VB, int SG, int MINB>
-__global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
-  constexpr int G = 32 / SG;
+// One task of the flagged walk by one sub-warp (sl = lane within the sub-warp, stage = its
+// 32-entry staging buffer).
+template <class T, class TA, class ACC, int VB, int SG>
+__device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, unsigned sgmask,
+                                          int2 *stage) {
   constexpr int UNR = 4;
-  __shared__ int2 stage_all[8 * G][32];
-  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
-  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
-  int2 *stage = stage_all[(threadIdx.x >> 5) * G + sg];
-  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
-  if (t >= a.ntasks) return;
   const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
   const int64_t d0 = (int64_t)t * a.U;
   const int p = (int)(d0 - hdr.x);
@@ -393,6 +391,58 @@ __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a
   }
   if (hdr.z >= 0 && hdr.x < hdr.y) arrive<T, ACC, VB, SG, 1>(a, hdr.z, sl, sgmask);
   if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1>(a, hdr.w, sl, sgmask);
+}
+
+template <class T, class TA, class ACC, int VB, int SG, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
+  constexpr int G = 32 / SG;
+  __shared__ int2 stage_all[8 * G][32];
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  flag_walk<T, TA, ACC, VB, SG>(a, t, sl, sgmask, stage_all[(threadIdx.x >> 5) * G + sg]);
+}
+
+// Batched products in one persistent launch: matrix i owns warp items
+// [item_off[i], item_off[i+1]), each item G_i = 32 / SG_i consecutive tasks of its plan; the
+// sub-warp width follows that matrix's N (16-byte vectors for N <= 128, or scalars for
+// N <= 32).  Warps stride over the items of all matrices; every matrix's split rows are
+// combined by its own counters exactly as in a single product.
+__global__ void __launch_bounds__(256, 4) merge_batch_kernel(const MergeArgs *__restrict__ args,
+                                                             const int *__restrict__ shape,
+                                                             const int64_t *__restrict__ item_off,
+                                                             int count) {
+  __shared__ int2 stage_all[8 * 4][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t total = __ldg(item_off + count);
+  const int64_t nw = (int64_t)gridDim.x * 8;
+  for (int64_t w = (int64_t)blockIdx.x * 8 + warp; w < total; w += nw) {
+    __syncwarp();
+    int lo = 0, hi = count;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(item_off + mid) <= w) lo = mid; else hi = mid;
+    }
+    const MergeArgs &a = args[lo];
+    const int item = (int)(w - __ldg(item_off + lo));
+    switch (__ldg(shape + lo)) {
+#define SW_BATCH_SHAPE(CODE, VB_, SG_)                                                          \
+  case CODE: {                                                                                  \
+    const int sg = lane / SG_, sl = lane % SG_;                                                 \
+    const unsigned m = SG_ == 32 ? 0xffffffffu : (((1u << SG_) - 1u) << (sg * SG_));            \
+    const int t = item * (32 / SG_) + sg;                                                       \
+    if (t < a.ntasks) flag_walk<float, float, float, VB_, SG_>(a, t, sl, m, stage_all[warp * 4 + sg]); \
+    break;                                                                                      \
+  }
+      SW_BATCH_SHAPE(0, 4, 8)
+      SW_BATCH_SHAPE(1, 4, 16)
+      SW_BATCH_SHAPE(2, 4, 32)
+      SW_BATCH_SHAPE(3, 1, 32)
+#undef SW_BATCH_SHAPE
+      default: break;
+    }
+  }
 }
 
 // Execution copy of the gather indices with bit 31 on the first nonzero of every row.
@@ -677,6 +727,67 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
     default: return SWIFT_ERR_UNSUPPORTED;
   }
 #undef SW_MDISPATCH
+}
+
+size_t merge_args_size() { return sizeof(MergeArgs); }
+
+// One member of a batch: tasks of U positions over the member's own layout L (which points at
+// the plan's CSR), scratch for N columns, and its launch record (FP32 plan, FP32 row-major B
+// and C).  shape selects the sub-warp width of merge_batch_kernel; items = warp items.
+swift_status merge_batch_member(const Plan &p, RowLayout &L, int U, int N, const void *B, int64_t ldb,
+                                void *C, int64_t ldc, void *args_out, int *shape, int64_t *items,
+                                cudaStream_t st) {
+  if (p.val_type != SWIFT_F32 || !p.has_csr || N < 0) return SWIFT_ERR_UNSUPPORTED;
+  const bool v16 = ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) && (ldb % 4 == 0) &&
+                   (ldc % 4 == 0) && (N % 4 == 0);
+  int sh, G;
+  if (v16 && N <= 128) {
+    sh = N <= 32 ? 0 : (N <= 64 ? 1 : 2);
+    G = sh == 0 ? 4 : (sh == 1 ? 2 : 1);
+  } else if (N <= 32) {
+    sh = 3;
+    G = 1;
+  } else {
+    set_last_error("swift_batch", "N above 128, or above 32 without 16-byte aligned operands");
+    return SWIFT_ERR_UNSUPPORTED;
+  }
+  L.rows = p.M; L.cols = p.K; L.nnz = p.nnz;
+  L.ptr = p.rowptr.as<int>(); L.idx = p.colidx.as<int>(); L.val = p.val.p; L.out_row = nullptr;
+  SW_TRY(build_merge_tasks(L, U, st));
+  const size_t need = (size_t)2 * L.ntasks * (size_t)N * sizeof(float);
+  if (need > L.mscratch.bytes) SW_TRY(L.mscratch.alloc(need));
+  MergeArgs a{};
+  a.rows = L.rows; a.N = N; a.U = L.merge_U; a.ntasks = (N == 0 || p.M == 0) ? 0 : L.ntasks;
+  a.total = (int64_t)L.nnz + L.rows;
+  a.ptr = L.ptr; a.idx = L.eidx.as<int>(); a.val = L.val; a.out_row = nullptr;
+  a.B = B; a.ldb = ldb; a.C = C; a.ldc = ldc;
+  a.task_row = L.task_row.as<int>(); a.head_split = L.head_split.as<int>(); a.tail_split = L.tail_split.as<int>();
+  a.task_hdr = L.task_hdr.as<int>();
+  a.split_row = L.split_row.as<int>(); a.split_first = L.split_first.as<int>();
+  a.split_last = L.split_last.as<int>(); a.split_cnt = L.split_cnt.as<int>();
+  a.scratch = L.mscratch.p;
+  std::memcpy(args_out, &a, sizeof(MergeArgs));
+  *shape = sh;
+  *items = ((int64_t)a.ntasks + G - 1) / G;
+  return SWIFT_OK;
+}
+
+// Persistent grid: every SM filled with as many 256-thread blocks as fit.
+swift_status merge_batch_grid(int device, int *grid) {
+  int sms = 0, per = 0;
+  SW_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  SW_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, merge_batch_kernel, 256, 0));
+  *grid = sms * std::max(per, 1);
+  return SWIFT_OK;
+}
+
+swift_status launch_merge_batch(const void *d_args, const int *d_shape, const int64_t *d_item_off,
+                                int count, int grid, cudaStream_t st) {
+  if (count <= 0 || grid <= 0) return SWIFT_OK;
+  merge_batch_kernel<<<grid, 256, 0, st>>>(static_cast<const MergeArgs *>(d_args), d_shape, d_item_off,
+                                           count);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
 }
 
 }  // namespace swift

@@ -142,6 +142,7 @@ _SIGS = [
     ("swift_batch_set_operands", C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     ("swift_batch_run", C.c_int, [_P, _P]),
     ("swift_batch_run_graph", C.c_int, [_P, _P]),
+    ("swift_batch_autotune", C.c_int, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
 ]
 # reference-convention functions (host buffers), one per value type
 _FP = C.POINTER(C.c_float)

@@ -122,6 +122,67 @@ def random_csr(M: int, K: int, density: float, seed: int = 0, skew: float = 0.0)
     return coo_to_csr(M, rows, cols, K=K)
 
 
+def rmat_rect(M: int, nedges: int, seed: int = 0, device="cpu"):
+    """R-MAT on the next power of two >= M with coordinates outside M x M rejected and
+    duplicates merged (torch; any device)."""
+    import torch
+
+    scale = max(1, int(np.ceil(np.log2(max(M, 2)))))
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    r = torch.zeros(nedges, dtype=torch.int64, device=device)
+    c = torch.zeros(nedges, dtype=torch.int64, device=device)
+    for lvl in range(scale):
+        u = torch.rand(nedges, generator=g, device=device)
+        sh = scale - 1 - lvl
+        r |= (u >= 0.76).to(torch.int64) << sh
+        c |= (((u >= 0.57) & (u < 0.76)) | (u >= 0.95)).to(torch.int64) << sh
+    keep = (r < M) & (c < M)
+    key = torch.unique(r[keep] * M + c[keep])
+    counts = torch.bincount(key // M, minlength=M)
+    rowptr = torch.zeros(M + 1, dtype=torch.int64, device=device)
+    rowptr[1:] = torch.cumsum(counts, 0)
+    return rowptr.to(torch.int32).cpu().numpy(), (key % M).to(torch.int32).cpu().numpy()
+
+
+def _uniform_rows(M: int, lam: float, seed: int, device="cpu"):
+    """M x M with ~Poisson(lam) row lengths and uniform columns (drawn with replacement and
+    merged, which removes under 3% of the draws at lam <= 64, M >= 1024); torch, any device."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    lens = torch.poisson(torch.full((M,), float(lam), device=device), generator=g).to(torch.int64)
+    rows = torch.repeat_interleave(torch.arange(M, device=device), lens.clamp(max=M))
+    cols = torch.randint(0, M, (rows.numel(),), generator=g, device=device)
+    key = torch.unique(rows * M + cols)
+    rowptr = torch.zeros(M + 1, dtype=torch.int64, device=device)
+    rowptr[1:] = torch.cumsum(torch.bincount(key // M, minlength=M), 0)
+    return rowptr.to(torch.int32).cpu().numpy(), (key % M).to(torch.int32).cpu().numpy()
+
+
+def batch_matrices(count: int, seed: int = 0, m_lo: int = 1024, m_hi: int = 65536, device="cpu"):
+    """The batching workload: square matrices with M log-uniform in [m_lo, m_hi] and average
+    degree U[4, 64]; the first half uniform-random (Poisson row lengths, uniform columns),
+    the second half R-MAT (a, b, c, d = .57, .19, .19, .05); each with its own dense width N
+    from {32, 64, 128}.  Returns a list of dicts (M, rowptr, colidx, N, kind)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        M = int(round(np.exp(rng.uniform(np.log(m_lo), np.log(m_hi)))))
+        deg = float(rng.uniform(4.0, 64.0))
+        N = int(rng.choice([32, 64, 128]))
+        s = int(rng.integers(0, 2**31 - 1))
+        if i < count // 2:
+            rp, ci = _uniform_rows(M, deg, s, device)
+            kind = "uniform"
+        else:
+            rp, ci = rmat_rect(M, int(round(deg * M)), seed=s, device=device)
+            kind = "rmat"
+        out.append(dict(M=M, rowptr=rp, colidx=ci, N=N, kind=kind))
+    return out
+
+
 def sym_normalized_values(rowptr: np.ndarray, colidx: np.ndarray, M: int, dtype=np.float32):
     """1 / sqrt(d_i d_j) for a (symmetric) pattern -- the graph-convolution weighting."""
     deg = np.diff(rowptr).astype(np.float64)

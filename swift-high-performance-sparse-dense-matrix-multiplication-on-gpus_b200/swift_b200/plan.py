@@ -243,3 +243,58 @@ class Plan:
                                                   C_out.data_ptr(), _stream_ptr(stream), C.byref(ms),
                                                   C.byref(eng)), "swift_plan_autotune")
         return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise"}[eng.value], ms.value
+
+
+class Batch:
+    """Independent products C_i = A_i @ B_i (FP32, row-major) in one persistent launch.
+
+        batch = Batch(plans)
+        batch.set_operands(Bs, Cs)     # CUDA tensors, one pair per plan
+        batch.run()                    # or batch.run_graph() (captured once, then replayed)
+    The plans must stay alive while the batch exists."""
+
+    def __init__(self, plans, stream=None):
+        self.plans = list(plans)
+        arr = (C.c_void_p * max(len(self.plans), 1))(*[p._h.value for p in self.plans])
+        h = C.c_void_p()
+        capi.check(capi.lib().swift_batch_create(arr, len(self.plans), _stream_ptr(stream), C.byref(h)),
+                   "swift_batch_create")
+        self._h = h
+        self._keep = None
+
+    def set_operands(self, Bs, Cs, stream=None):
+        n = len(self.plans)
+        if len(Bs) != n or len(Cs) != n:
+            raise ValueError("one B and one C per plan")
+        Ns = (C.c_int * max(n, 1))(*[int(b.shape[1]) for b in Bs])
+        Bp = (C.c_void_p * max(n, 1))(*[b.data_ptr() for b in Bs])
+        Cp = (C.c_void_p * max(n, 1))(*[c.data_ptr() for c in Cs])
+        ldb = (C.c_int64 * max(n, 1))(*[_ld(b, capi.ROW_MAJOR) for b in Bs])
+        ldc = (C.c_int64 * max(n, 1))(*[_ld(c, capi.ROW_MAJOR) for c in Cs])
+        capi.check(capi.lib().swift_batch_set_operands(self._h, Ns, Bp, ldb, Cp, ldc, _stream_ptr(stream)),
+                   "swift_batch_set_operands")
+        self._keep = (list(Bs), list(Cs))
+
+    def run(self, stream=None):
+        capi.check(capi.lib().swift_batch_run(self._h, _stream_ptr(stream)), "swift_batch_run")
+
+    def run_graph(self, stream=None):
+        capi.check(capi.lib().swift_batch_run_graph(self._h, _stream_ptr(stream)), "swift_batch_run_graph")
+
+    def autotune(self, stream=None):
+        """Chooses the task size over the whole batch; returns (task_size, ms per run)."""
+        ms, U = C.c_double(0), C.c_int(0)
+        capi.check(capi.lib().swift_batch_autotune(self._h, _stream_ptr(stream), C.byref(ms), C.byref(U)),
+                   "swift_batch_autotune")
+        return U.value, ms.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            capi.lib().swift_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
