@@ -8,8 +8,10 @@
  *
  * All entry points are plain C: pointers, sizes and enums only.  Every call returns a
  * swift_status; nothing prints and nothing exits.  Device work is stream-ordered on the
- * caller's stream (NULL = the legacy default stream).  Plans are immutable after creation
- * and may be used concurrently from several streams.
+ * caller's stream (NULL = the legacy default stream).  A plan's pattern is fixed at
+ * creation; its products share per-plan scratch (split-row partials and counters), so the
+ * products of one plan must be ordered on one stream (or separated by events); different
+ * plans run concurrently without restriction.
  *
  * Reference interface each entry point replaces (paths inside the reference project):
  *   swift_plan_create           -- csr_to_csc + col_sort/ColSort + formattransation/
@@ -27,9 +29,9 @@
  *   swift_ref_*                 -- the same functions with the reference's host-buffer
  *                                  calling convention (see swift_compat.h for the C++ shims
  *                                  that carry the reference's exact signatures)
- *   swift_spmm_transposed, swift_sddmm, swift_fused_forward_backward, swift_batch_*
- *                               -- no counterpart in the reference (backward pass and
- *                                  batched execution added by this library)
+ *   swift_spmm_transposed, swift_sddmm, swift_fused_forward_backward, swift_batch_*,
+ *   swift_plan_set_values       -- no counterpart in the reference (backward pass, batched
+ *                                  execution and value updates added by this library)
  */
 #ifndef SWIFT_B200_H
 #define SWIFT_B200_H
@@ -172,6 +174,13 @@ swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
                                swift_stream_t stream, swift_plan **out);
 swift_status swift_plan_destroy(swift_plan *plan);
 swift_status swift_plan_get_stats(const swift_plan *plan, swift_plan_stats *out);
+/* New values for the plan's fixed pattern (nnz values of the plan's value type, CSR order,
+ * host or device memory); every value copy of the format is refilled on `stream`, the
+ * pattern, column order and task layouts are kept.  No counterpart in the reference (added
+ * for training loops that update A's values).  Products already queued on other streams
+ * must have finished. */
+swift_status swift_plan_set_values(swift_plan *plan, const void *val, swift_memspace mem,
+                                   swift_stream_t stream);
 
 /* Host copies of every reference array.  with_row_sort != 0 also runs the per-8-tile row
  * sort (src/back_process.h:23-229) and fills val_position / val_offset; the reference

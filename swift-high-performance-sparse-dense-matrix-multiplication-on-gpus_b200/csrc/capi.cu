@@ -191,6 +191,20 @@ swift_status swift_plan_get_stats(const swift_plan *plan, swift_plan_stats *o) {
   return SWIFT_OK;
 }
 
+swift_status swift_plan_set_values(swift_plan *plan, const void *val, swift_memspace mem,
+                                   swift_stream_t stream) {
+  if (!plan || (mem != SWIFT_HOST && mem != SWIFT_DEVICE)) return SWIFT_ERR_INVALID_ARG;
+  Plan &p = plan->p;
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  if (p.nnz > 0 && !val) return SWIFT_ERR_INVALID_ARG;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  std::lock_guard<std::mutex> g(p.mu);
+  if (p.nnz > 0)
+    SW_CHECK_CUDA(cudaMemcpyAsync(p.val.p, val, p.vsz * (size_t)p.nnz,
+                                  mem == SWIFT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  return refresh_values(p, st);
+}
+
 swift_status swift_plan_export_f32(const swift_plan *plan, swift_slide_matrix_f32 *out,
                                    int with_row_sort, float *blockratio) {
   if (!plan || !out) return SWIFT_ERR_INVALID_ARG;

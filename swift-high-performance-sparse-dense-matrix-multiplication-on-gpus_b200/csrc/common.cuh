@@ -210,6 +210,8 @@ swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *
 // Steps, tiles, reside and balance from a device-resident sorted CSC already in the plan
 // (p.sortnnz, p.sptr, p.srow, p.sval).
 swift_status build_tiles(Plan &p, cudaStream_t st);
+// New CSR-order values already in p.val: refills the sorted CSC values, tile slots, reside part.
+swift_status refresh_values(Plan &p, cudaStream_t st);
 // Tiled-engine work items from tile_colidx (also used for plans made from a slide_matrix).
 swift_status build_items(Plan &p, cudaStream_t st);
 // Balance blocks from p.reside_ptr (device) and its host copy.

@@ -744,6 +744,52 @@ swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *
   return build_tiles(p, st);
 }
 
+namespace {
+template <class T>
+__global__ void value_gather_kernel(const int *__restrict__ spos, const T *__restrict__ val, int64_t nnz,
+                                    T *__restrict__ sval) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz;
+       q += (int64_t)gridDim.x * blockDim.x)
+    sval[q] = val[spos[q]];
+}
+
+template <class T>
+swift_status refresh_typed(Plan &p, cudaStream_t st) {
+  if (p.nnz > 0) {
+    value_gather_kernel<T><<<grid_for(p.nnz), 256, 0, st>>>(p.spos.as<int>(), p.val.as<T>(), p.nnz,
+                                                             p.sval.as<T>());
+    SW_CHECK_LAUNCH();
+  }
+  if (p.tilenum > 0) {
+    TmpBuf fmt;
+    SW_TRY(fmt.alloc(sizeof(int) * 4, st));
+    SW_CHECK_CUDA(cudaMemsetAsync(fmt.p, 0, sizeof(int) * 4, st));
+    tile_fill_kernel<T><<<grid_for((int64_t)p.tilenum * 32, 256, 148 * 32), 256, 0, st>>>(
+        p.tilenum, p.nsteps, p.step_tile_off.as<int>(), p.step_col.as<int>(), p.step_base.as<int>(),
+        p.step_tall.as<int>(), p.sptr.as<int>(), p.srow.as<int>(), p.sval.as<T>(), p.tile_colidx.as<int>(),
+        p.tile_depth.as<int>(), p.tile_tall.as<int>(), p.tile_format.as<int>(), p.sortrowidx.as<int>(),
+        p.sortval.as<T>(), fmt.as<int>());
+    SW_CHECK_LAUNCH();
+  }
+  if (p.reside_col > 0) {
+    reside_fill_kernel<T><<<p.reside_col, 256, 0, st>>>(
+        p.K, p.nsteps, p.sortnnz.as<int>(), p.sptr.as<int>(), p.srow.as<int>(), p.sval.as<T>(),
+        p.step_col.as<int>(), p.step_base.as<int>(), p.reside_ptr.as<int>(), p.reside_row.as<int>(),
+        p.reside_val.as<T>());
+    SW_CHECK_LAUNCH();
+  }
+  return SWIFT_OK;
+}
+}  // namespace
+
+// New values for the plan's fixed pattern (CSR order, already in p.val): the sorted CSC
+// values, the tile slots and the reside part are refilled from it; pattern arrays, the
+// column order and every row layout stay as built.
+swift_status refresh_values(Plan &p, cudaStream_t st) {
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  return p.val_type == SWIFT_F64 ? refresh_typed<double>(p, st) : refresh_typed<float>(p, st);
+}
+
 // ---------------------------------------------------------------------------------------------
 swift_status build_row_layout(Plan &p, RowLayout &L, bool transpose, cudaStream_t st) {
   if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;

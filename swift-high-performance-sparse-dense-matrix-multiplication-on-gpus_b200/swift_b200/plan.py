@@ -127,6 +127,27 @@ class Plan:
         d["fmt_count"] = list(s.fmt_count)
         return d
 
+    def set_values(self, val, stream=None):
+        """New values for the fixed pattern (CSR order; numpy or a CUDA tensor of the plan's
+        value type)."""
+        torch = _torch()
+        if isinstance(val, torch.Tensor) and val.is_cuda:
+            want = torch.float64 if self.val_dtype == np.float64 else torch.float32
+            v = val.detach()
+            if v.dtype != want or not v.is_contiguous():
+                v = v.to(want).contiguous()
+            if v.numel() != self.nnz:
+                raise ValueError(f"{v.numel()} values for {self.nnz} nonzeros")
+            capi.check(capi.lib().swift_plan_set_values(self._h, v.data_ptr(), capi.DEVICE, _stream_ptr(stream)),
+                       "swift_plan_set_values")
+            self._vals_in_flight = v  # the copy is stream-ordered: keep the source alive
+        else:
+            v = np.ascontiguousarray(val, self.val_dtype)
+            if v.size != self.nnz:
+                raise ValueError(f"{v.size} values for {self.nnz} nonzeros")
+            capi.check(capi.lib().swift_plan_set_values(self._h, v.ctypes.data if v.size else None, capi.HOST,
+                                                        _stream_ptr(stream)), "swift_plan_set_values")
+
     def export(self, with_row_sort=False) -> dict:
         """Every reference slide_matrix array as numpy (host copies made on the GPU)."""
         f64 = self.val_dtype == np.float64
