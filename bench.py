@@ -39,12 +39,12 @@ WORKLOADS = {
     "rmat20_n32_f64": dict(kind="rmat", scale=20, edges=16 << 20, N=32, dtype="f64"),
     # half-size case for full ncu captures (B and C still exceed L2)
     "rmat19_n128_f32": dict(kind="rmat", scale=19, edges=8 << 20, N=128, dtype="f32"),
-    # half-size case for full ncu captures (B and C still exceed L2)
-    "rmat19_n128_f32": dict(kind="rmat", scale=19, edges=8 << 20, N=128, dtype="f32"),
     # precision workload: R-MAT scale 19 avg degree 32 merged with a 64-wide band, 16-bit B/C
     "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
     "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),
     "rmat19band_n128_f32": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f32"),
+    # the batching workload: 512 independent products in one persistent launch
+    "batch512_f32": dict(kind="batch", count=512, N=None, dtype="f32"),
     # the 4096 x 4096 parity workload (rows ~Poisson(16))
     "poisson4096_n32_f32": dict(kind="poisson", M=4096, K=4096, lam=16.0, N=32, dtype="f32"),
 }
@@ -233,10 +233,128 @@ def run_cpu_samples(cs, seconds, warm=1):
 
 
 # ------------------------------------------------------------------------------------ ours
+def run_batch(args):
+    """The batching workload: 512 independent products in one persistent launch, replayed as
+    a CUDA graph; value = the batch's total GFLOP/s."""
+    import torch
+
+    from swift_b200 import Batch, Plan, gen
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    wl = WORKLOADS[args.workload]
+    mats = gen.batch_matrices(wl["count"], seed=0, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    plans, Bs, Cs = [], [], []
+    flops = alg_bytes = 0
+    nnz_tot = rows_tot = 0
+    for i, m in enumerate(mats):
+        M, N = m["M"], m["N"]
+        nnz = int(m["rowptr"][-1])
+        val = torch.rand(nnz, generator=g, device="cuda") * 2 - 1
+        plans.append(Plan.from_csr(torch.from_numpy(m["rowptr"]).cuda(), torch.from_numpy(m["colidx"]).cuda(),
+                                   val, (M, M)))
+        Bs.append(torch.rand((M, N), generator=g, device="cuda") * 2 - 1)
+        Cs.append(torch.empty((M, N), device="cuda"))
+        flops += 2.0 * nnz * N
+        alg_bytes += nnz * 8 + 2 * M * N * 4
+        nnz_tot += nnz
+        rows_tot += M
+    batch = Batch(plans)
+    batch.set_operands(Bs, Cs)
+    best_U, tune_ms = batch.autotune()
+    for _ in range(args.warmup):
+        batch.run_graph()
+    stream = torch.cuda.current_stream()
+    gpu_idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[local] if os.environ.get("CUDA_VISIBLE_DEVICES") else local
+    sampler = ClockSampler(gpu_idx)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.run_graph()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop(w0, time.time())
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * flops * args.steps / (ms / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    # end to end: every member's B in from pinned host memory, every C out, one launch
+    Bh = [b.cpu().pin_memory() for b in Bs]
+    Ch = [torch.empty(c.shape, dtype=c.dtype).pin_memory() for c in Cs]
+    h2d = sum(b.numel() * 4 for b in Bh)
+    d2h = sum(c.numel() * 4 for c in Ch)
+    n_e2e = max(1, min(args.e2e_steps, 3))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(n_e2e):
+        for b, bh in zip(Bs, Bh):
+            b.copy_(bh, non_blocking=True)
+        batch.run_graph()
+        for c, ch in zip(Cs, Ch):
+            ch.copy_(c, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    Ns = [m["N"] for m in mats]
+    out = {
+        "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator; 512 square matrices, M log-uniform in [1024, 65536], "
+                "average degree U[4, 64], half uniform-random and half R-MAT; N from {32, 64, 128})",
+        "config": {"workload": args.workload, "matrices": len(mats), "rows": rows_tot, "nnz": nnz_tot,
+                   "N_counts": {str(n): Ns.count(n) for n in (32, 64, 128)}, "task_size": best_U,
+                   "autotune_ms": tune_ms, "launch": "one persistent kernel per step, replayed as a CUDA graph",
+                   "l2": "B and C of the batch (about 5 GB) exceed L2; no flush between steps",
+                   "parallelism": f"replicas x{world} (no exchange step)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind, "kernel": "merge_batch_kernel",
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "e2e": {"value": world * flops * n_e2e / (e2e_ms / 1e3) / 1e9, "unit": "GFLOP/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": n_e2e,
+                "ms_per_step": e2e_ms / n_e2e},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "cpu_baseline": None,
+    }
+    print(json.dumps(out), flush=True)
+    batch.close()
+
+
 def run_ours(args):
     import torch
 
     from swift_b200 import Plan
+    if WORKLOADS[args.workload]["kind"] == "batch":
+        return run_batch(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -257,6 +375,7 @@ def run_ours(args):
     plan = Plan.from_csr(d_rp, d_ci, val, (M, K))
     C = torch.empty((M, N), dtype=B.dtype, device="cuda")
     engine, tune_ms = plan.autotune(B, C)
+    rw_params = plan.rowwise_params(N, B.dtype) if engine == "rowwise" else None
     st = plan.stats()
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -312,24 +431,52 @@ def run_ours(args):
                  "hbm_frac_of_measured": alg_bytes / (t_ms / 1e3) / 1e9 / peak}
         plan.spmm(B, C)
 
-    # end to end: B from pinned host memory in, C back out, through the public call
-    Bh = B.cpu().pin_memory()
-    Ch = torch.empty((M, N), dtype=C.dtype).pin_memory()
-    for _ in range(1):
-        B.copy_(Bh, non_blocking=True)
-        plan.spmm(B, C)
-        Ch.copy_(C, non_blocking=True)
+    # end to end through the public call: every step copies its B in from pinned host memory
+    # and its C out to pinned host memory.  Copies in, products and copies out run on three
+    # streams over two device buffer sets, so step i's C leaves while step i+1's B arrives
+    # (PCIe is full duplex); the products stay ordered on one stream (one plan).
+    Bh = [B.cpu().pin_memory() for _ in range(2)]
+    Ch = [torch.empty((M, N), dtype=C.dtype).pin_memory() for _ in range(2)]
+    Bd = [B, torch.empty_like(B)]
+    Cd = [C, torch.empty_like(C)]
+    s_in, s_c, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_c = [torch.cuda.Event() for _ in range(2)]
+    ev_out = [torch.cuda.Event() for _ in range(2)]
+
+    def e2e_steps(n):
+        for i in range(n):
+            j = i % 2
+            with torch.cuda.stream(s_in):
+                if i >= 2:
+                    s_in.wait_event(ev_c[j])  # Bd[j] free once its product ran
+                Bd[j].copy_(Bh[j], non_blocking=True)
+                ev_in[j].record(s_in)
+            s_c.wait_event(ev_in[j])
+            if i >= 2:
+                s_c.wait_event(ev_out[j])  # Cd[j] free once it was copied out
+            plan.spmm(Bd[j], Cd[j], stream=s_c)
+            ev_c[j].record(s_c)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_c[j])
+                Ch[j].copy_(Cd[j], non_blocking=True)
+                ev_out[j].record(s_out)
+
+    torch.cuda.synchronize()
+    e2e_steps(2)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        B.copy_(Bh, non_blocking=True)
-        plan.spmm(B, C)
-        Ch.copy_(C, non_blocking=True)
-    e1.record(stream)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(s_in)
+    s_c.wait_event(t0)
+    s_out.wait_event(t0)
+    e2e_steps(args.e2e_steps)
+    s_out.wait_stream(s_in)
+    s_out.wait_stream(s_c)
+    t1.record(s_out)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = t0.elapsed_time(t1)
     if dist:
         t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -363,6 +510,7 @@ def run_ours(args):
         "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
         "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz),
                    "rows": M, "cols": K, "nnz": nnz, "N": N, "engine": engine,
+                   "row_engine_params": rw_params,
                    "parallelism": f"replicas x{world} (no exchange step)",
                    "l2": "inputs larger than L2 (B and C exceed 126 MB); no flush between steps",
                    "plan_build_ms": st["build_ms"], "autotune_ms": tune_ms,
@@ -374,9 +522,11 @@ def run_ours(args):
                      "kernel": kernel, "algorithmic_bytes_per_launch": alg_bytes,
                      "traffic_source": prof.get("file"),
                      "frac_of_8TBs_nominal": achieved / 8000.0},
-        "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": int(Bh.numel() * Bh.element_size()),
-                "d2h_bytes_per_step": int(Ch.numel() * Ch.element_size()), "steps": args.e2e_steps,
-                "ms_per_step": e2e_ms / args.e2e_steps},
+        "e2e": {"value": e2e_value, "unit": "GFLOP/s",
+                "h2d_bytes_per_step": int(Bh[0].numel() * Bh[0].element_size()),
+                "d2h_bytes_per_step": int(Ch[0].numel() * Ch[0].element_size()), "steps": args.e2e_steps,
+                "ms_per_step": e2e_ms / args.e2e_steps,
+                "pipeline": "H2D / product / D2H on three streams, two buffer sets"},
         "gpu_launches": args.steps * (1 if engine == "rowwise" else 2),
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -399,6 +549,8 @@ def run_reference(args):
         dev = "cuda" if torch.cuda.is_available() else "cpu"
     except Exception:
         dev = "cpu"
+    if wl["kind"] == "batch":
+        return run_reference_batch(args, wl, dev)
     M, K, rp, ci, val, B = make_inputs(wl, dev)
     import torch
     Bn = B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy()
@@ -440,6 +592,42 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_reference_batch(args, wl, dev):
+    """The reference's Swift_cpu over the batch members in order (whole products), until the
+    time budget is spent; value = flops of the products run / their time."""
+    from swift_b200 import gen
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    mats = gen.batch_matrices(wl["count"], seed=0, device=dev)
+    rng = np.random.default_rng(1)
+    tot_s = tot_f = 0.0
+    done = 0
+    kind = "ref"
+    for m in mats:
+        M, N = m["M"], m["N"]
+        nnz = int(m["rowptr"][-1])
+        val = rng.uniform(-1, 1, nnz).astype(np.float32)
+        B = rng.uniform(-1, 1, (M, N)).astype(np.float32)
+        cs, kind = cpu_swift(M, M, m["rowptr"], m["colidx"], val, B, N, impl="ref")
+        sec, n = cs.run(0, cs.tilenum, with_reside=True)
+        tot_s += sec
+        tot_f += 2.0 * n * N
+        done += 1
+        if tot_s >= args.ref_seconds:
+            break
+    value = tot_f / tot_s / 1e9 if tot_s > 0 else 0.0
+    sample = f"Swift_cpu over whole products of the first {done} of {len(mats)} matrices in {tot_s:.2f} s"
+    out = {
+        "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": done,
+        "warmup": 0, "ms_per_step": tot_s * 1e3 / max(1, done), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "impl": "reference", "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "matrices": len(mats), "parallelism": "host CPU, rank 0 only"},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": 1,
+                         "kind": "reference" if kind == "ref" else "port", "sample": sample},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -447,7 +635,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points of libswiftb200.so (declared in include/swift_b200.h).
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 
@@ -385,24 +386,36 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
   }
   const bool saved_override = p.merge_override;
   const MergeOpts saved_opts = p.merge_opts;
-  double best = 1e300;
-  Cand win{SWIFT_ENGINE_TILED, MergeOpts{}};
-  for (const Cand &c : cands) {
+  // ms per product of candidate c over `reps` launches (after warm-up), or < 0 if it fails
+  auto time_cand = [&](const Cand &c, int warm, int reps) -> double {
     p.merge_override = true;
     p.merge_opts = c.mo;
     swift_status rc = SWIFT_OK;
-    for (int w = 0; w < 2 && rc == SWIFT_OK; ++w)
+    for (int w = 0; w < warm && rc == SWIFT_OK; ++w)
       rc = swift_spmm(plan, c.eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
-    if (rc != SWIFT_OK) continue;
-    const int reps = 5;
+    if (rc != SWIFT_OK) return -1.0;
     cudaEventRecord(e0, st);
     for (int r = 0; r < reps; ++r)
       swift_spmm(plan, c.eng, N, dtype, B, N, SWIFT_ROW_MAJOR, 0, C, N, SWIFT_ROW_MAJOR, stream);
     cudaEventRecord(e1, st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -1.0;
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    if (ms / reps < best) { best = ms / reps; win = c; }
+    return ms / reps;
+  };
+  // a short pass over every candidate, then a longer one over the three fastest (the
+  // candidates differ by a few per cent, about the noise of a short pass)
+  std::vector<std::pair<double, size_t>> first;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    const double ms = time_cand(cands[i], 2, 5);
+    if (ms >= 0) first.push_back({ms, i});
+  }
+  std::sort(first.begin(), first.end());
+  double best = 1e300;
+  Cand win{SWIFT_ENGINE_TILED, MergeOpts{}};
+  for (size_t k = 0; k < first.size() && k < 3; ++k) {
+    const double ms = time_cand(cands[first[k].second], 1, 20);
+    if (ms >= 0 && ms < best) { best = ms; win = cands[first[k].second]; }
   }
   p.merge_override = saved_override;
   p.merge_opts = saved_opts;
