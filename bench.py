@@ -43,6 +43,10 @@ WORKLOADS = {
     "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
     "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),
     "rmat19band_n128_f32": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f32"),
+    # precision ratios (FP32 vs BF16 vs FP16 B/C on one FP32-valued matrix)
+    "precision_rmat19band_n128": dict(kind="precision", rk="rmatband", scale=19, edges=16 << 20, N=128),
+    # differentiation: GNN layer on a symmetric-normalised R-MAT graph, fused vs plain
+    "fwdbwd_rmat18sym_n64": dict(kind="fwdbwd", scale=18, edges=(32 << 18) // 2, N=64, dtype="f32"),
     # the batching workload: 512 independent products in one persistent launch
     "batch512_f32": dict(kind="batch", count=512, N=None, dtype="f32"),
     # the 4096 x 4096 parity workload (rows ~Poisson(16))
@@ -233,6 +237,128 @@ def run_cpu_samples(cs, seconds, warm=1):
 
 
 # ------------------------------------------------------------------------------------ ours
+def _timed(fn, steps, warmup):
+    """Device ms per call of fn (CUDA events on the current stream, after warm-up)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _single_gpu_line(args, out):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_precision(args):
+    """The precision workload: one FP32-valued plan, products with FP32, BF16 and FP16 B and C
+    (FP32 accumulation); value = BF16 GFLOP/s; ratios against FP32 and errors against the
+    deterministic FP64 product beside it."""
+    import torch
+
+    from swift_b200 import Plan
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    M, K, rp, ci, val, B32 = make_inputs(dict(wl, kind="rmatband", dtype="f32"), "cuda")
+    N = wl["N"]
+    nnz = int(rp[-1])
+    plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
+    ref = plan.spmm_f64_reference(B32.double())
+    refmax = ref.abs().max().item()
+    res = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+        B = B32.to(dt)
+        C = torch.empty((M, N), dtype=dt, device="cuda")
+        eng, _ = plan.autotune(B, C)
+        ms = _timed(lambda: plan.spmm(B, C), args.steps, args.warmup)
+        plan.spmm(B, C)
+        err = (C.double() - ref).abs().max().item() / refmax
+        # error of the 16-bit result against the same product on 16-bit-rounded inputs in FP64
+        err_in = None
+        if dt != torch.float32:
+            ref_q = plan.spmm_f64_reference(B.double())
+            err_in = (C.double() - ref_q).abs().max().item() / ref_q.abs().max().item()
+        bytes_ = nnz * 8 + (K + M) * N * B.element_size()
+        res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": eng,
+                     "err_vs_fp64": err, "err_vs_fp64_on_rounded_B": err_in,
+                     "algorithmic_bytes": bytes_, "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / hbm_peak()[0]}
+    f32b, bfb = res["f32"]["algorithmic_bytes"], res["bf16"]["algorithmic_bytes"]
+    out = {
+        "metric": "spmm_gflops", "value": res["bf16"]["gflops"], "unit": "GFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["bf16"]["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 B/C, fp32 accumulate", "data": "synthetic",
+        "config": {"workload": args.workload, "rows": M, "nnz_realised": nnz, "N": N,
+                   "description": describe(args.workload, dict(wl, kind="rmatband", dtype="bf16/f16/f32"), nnz)},
+        "ratio_bf16_vs_f32": res["f32"]["ms"] / res["bf16"]["ms"],
+        "ratio_f16_vs_f32": res["f32"]["ms"] / res["f16"]["ms"],
+        "byte_model_ceiling_16bit_vs_f32": f32b / bfb,
+        "products": res,
+    }
+    _single_gpu_line(args, out)
+
+
+def run_fwdbwd(args):
+    """The differentiation workload: Y = A X, dX = A^T dY, dA = SDDMM(dY, X) on a symmetric-
+    normalised R-MAT graph; fused (one pass over A for Y and dA, then A^T) against the same
+    three products run separately; value = fused GFLOP/s (3 x 2 nnz N per step)."""
+    import torch
+
+    from swift_b200 import Plan, gen
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    rp, ci = gen.rmat(wl["scale"], wl["edges"], seed=0, device="cuda", symmetric=True, self_loops=False)
+    M = 1 << wl["scale"]
+    N = wl["N"]
+    nnz = int(rp[-1])
+    vals = gen.sym_normalized_values(rp, ci, M, np.float32)
+    plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), torch.from_numpy(vals).cuda(),
+                         (M, M), build_transpose=True)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    X = torch.randn((M, N), generator=g, device="cuda")
+    dY = torch.randn((M, N), generator=g, device="cuda")
+    Y = torch.empty_like(X)
+    dX = torch.empty_like(X)
+    dA = torch.empty(nnz, device="cuda")
+    plan.autotune(X, Y)
+
+    def plain():
+        plan.spmm(X, Y)
+        plan.spmm_t(dY, dX)
+        plan.sddmm(dY, X, dA)
+
+    def fused():
+        plan.fused_forward_backward(X, dY, Y, dX, dA)
+
+    t_plain = _timed(plain, args.steps, args.warmup)
+    t_fused = _timed(fused, args.steps, args.warmup)
+    t_fwd = _timed(lambda: plan.spmm(X, Y), args.steps, args.warmup)
+    t_bwd = _timed(lambda: plan.spmm_t(dY, dX), args.steps, args.warmup)
+    t_sddmm = _timed(lambda: plan.sddmm(dY, X, dA), args.steps, args.warmup)
+    flops = 3 * 2.0 * nnz * N
+    out = {
+        "metric": "spmm_gflops", "value": flops / (t_fused / 1e3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fused, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "nodes": M, "nnz": nnz, "N": N,
+                   "graph": f"R-MAT scale {wl['scale']} symmetrised, no self loops, values 1/sqrt(d_i d_j)"},
+        "ratio_fused_vs_plain": t_plain / t_fused,
+        "ms": {"plain_fwd_bwd": t_plain, "fused_fwd_bwd": t_fused, "spmm": t_fwd, "spmm_transposed": t_bwd,
+               "sddmm": t_sddmm},
+    }
+    _single_gpu_line(args, out)
+
+
 def run_batch(args):
     """The batching workload: 512 independent products in one persistent launch, replayed as
     a CUDA graph; value = the batch's total GFLOP/s."""
@@ -353,8 +479,13 @@ def run_ours(args):
     import torch
 
     from swift_b200 import Plan
-    if WORKLOADS[args.workload]["kind"] == "batch":
+    kind = WORKLOADS[args.workload]["kind"]
+    if kind == "batch":
         return run_batch(args)
+    if kind == "precision":
+        return run_precision(args)
+    if kind == "fwdbwd":
+        return run_fwdbwd(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
