@@ -319,6 +319,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
     }
     pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
   };
+  auto accumulate = [&](float wf, const BVec<T, ACC, VB> &b) { b.template fma_into<true>(acc, (ACC)wf); };
   const char *Bl = reinterpret_cast<const char *>(static_cast<const T *>(a.B) + sl * VB);
   const int64_t ldb_bytes = a.ldb * (int64_t)sizeof(T);
   const TA *val = static_cast<const TA *>(a.val);
@@ -338,48 +339,34 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
     if (m == 32) {
 #pragma unroll 1
       for (int k = 0; k < 32; k += UNR) {
-        ACC b[UNR][VB];
+        BVec<T, ACC, VB> b[UNR];
         int flags = 0;
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
           const int c = stage[k + u].x;
           flags |= c;
-          if (inb) vload<T, ACC, VB>(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes), b[u]);
-          else {
-#pragma unroll
-            for (int e = 0; e < VB; ++e) b[u][e] = ACC(0);
-          }
+          if (inb) b[u].load(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes));
+          else b[u].zero();
         }
         if (flags < 0) {
 #pragma unroll
           for (int u = 0; u < UNR; ++u) {
             while (q0 + k + u == pe) finish_and_advance();
-            const ACC w = (ACC)__int_as_float(stage[k + u].y);
-#pragma unroll
-            for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+            accumulate(__int_as_float(stage[k + u].y), b[u]);
           }
         } else {
 #pragma unroll
-          for (int u = 0; u < UNR; ++u) {
-            const ACC w = (ACC)__int_as_float(stage[k + u].y);
-#pragma unroll
-            for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
-          }
+          for (int u = 0; u < UNR; ++u) accumulate(__int_as_float(stage[k + u].y), b[u]);
         }
       }
     } else {
       for (int k = 0; k < m; ++k) {
         const int c = stage[k].x;
-        ACC b[VB];
-        if (inb) vload<T, ACC, VB>(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes), b);
-        else {
-#pragma unroll
-          for (int e = 0; e < VB; ++e) b[e] = ACC(0);
-        }
+        BVec<T, ACC, VB> b;
+        if (inb) b.load(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes));
+        else b.zero();
         while (q0 + k == pe) finish_and_advance();
-        const ACC w = (ACC)__int_as_float(stage[k].y);
-#pragma unroll
-        for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[e], acc[e]);
+        accumulate(__int_as_float(stage[k].y), b);
       }
     }
   }
@@ -582,6 +569,14 @@ constexpr int lean_minb(int VB, int AB, int UNR) {
   return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
+// The flagged walk keeps 4 gathered vectors in their stored width (TB bytes per element) and
+// the accumulators in AB bytes per element.
+constexpr int flag_minb(int VB, int AB, int TB) {
+  const int regs = 28 + VB * AB / 4 + 4 * ((VB * TB + 3) / 4);
+  const int b = 65536 / (256 * regs);
+  return b < 1 ? 1 : (b > 8 ? 8 : b);
+}
+
 template <class T, class TA, class ACC, int VB, int SG, int MINB>
 swift_status launch_flag(MergeArgs a, const int *eidx, cudaStream_t st) {
   constexpr int G = 32 / SG;
@@ -614,7 +609,7 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   // flagged-index kernel (FP32-valued plans): 4 loads in flight
 #define SW_MCASE_FLAG(VB_, SG_)                                                                 \
   if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_)                                   \
-    return launch_flag<T, TA, ACC, VB_, SG_, lean_minb(VB_, AB, 4)>(a, eidx, st);
+    return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T))>(a, eidx, st);
   if (sizeof(TA) == 4 && (kernel == 2 || (kernel == 0 && unr <= 4))) {
     SW_MCASE_FLAG(W, 2)
     SW_MCASE_FLAG(W, 4)

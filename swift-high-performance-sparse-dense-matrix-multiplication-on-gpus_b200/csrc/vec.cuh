@@ -84,6 +84,111 @@ __device__ __forceinline__ void vstore(T *__restrict__ p, const ACC (&a)[VB]) {
   }
 }
 
+// acc += w * b over one vector.  FP32 pairs go through the packed two-lane FMA of sm_100
+// (fma.rn.f32x2: each lane an IEEE fused multiply-add, so results equal the scalar form) to
+// halve the FMA instructions per gathered element.
+template <class ACC, int VB>
+__device__ __forceinline__ void fma_vec(ACC (&acc)[VB], ACC w, const ACC (&b)[VB]) {
+  if constexpr (sizeof(ACC) == 4 && VB % 2 == 0) {
+    unsigned long long ww;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(ww) : "f"(w));
+#pragma unroll
+    for (int e = 0; e < VB; e += 2) {
+      unsigned long long a2, b2;
+      asm("mov.b64 %0, {%1, %2};" : "=l"(a2) : "f"(acc[e]), "f"(acc[e + 1]));
+      asm("mov.b64 %0, {%1, %2};" : "=l"(b2) : "f"(b[e]), "f"(b[e + 1]));
+      asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(a2) : "l"(ww), "l"(b2));
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(acc[e]), "=f"(acc[e + 1]) : "l"(a2));
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[e], acc[e]);
+  }
+}
+
+// One gathered B vector held until it is consumed.  FP32/FP64 keep the converted values;
+// 16-bit types keep the raw packed words (half the registers while loads are in flight) and
+// convert a pair at a time when accumulating.
+template <class T, class ACC, int VB>
+struct BVec {
+  ACC v[VB];
+  __device__ __forceinline__ void load(const T *p) { vload<T, ACC, VB>(p, v); }
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int e = 0; e < VB; ++e) v[e] = ACC(0);
+  }
+  template <bool PK>
+  __device__ __forceinline__ void fma_into(ACC (&acc)[VB], ACC w) const {
+    if constexpr (PK) {
+      fma_vec<ACC, VB>(acc, w, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < VB; ++e) acc[e] = fma(w, v[e], acc[e]);
+    }
+  }
+};
+
+template <class T> __device__ __forceinline__ float2 unpack2(unsigned u);
+template <> __device__ __forceinline__ float2 unpack2<__nv_bfloat16>(unsigned u) {
+  return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u));
+}
+template <> __device__ __forceinline__ float2 unpack2<__half>(unsigned u) {
+  return __half22float2(*reinterpret_cast<const __half2 *>(&u));
+}
+
+template <class T, int VB>
+struct BVec16 {
+  static_assert(VB == 8 || VB == 16, "16-bit vectors of 16 or 32 bytes");
+  unsigned u[VB / 2];
+  __device__ __forceinline__ void load(const T *p) {
+    if constexpr (VB == 16) {
+      ld_nc_v8(p, u);
+    } else {
+      const uint4 q = __ldg(reinterpret_cast<const uint4 *>(p));
+      u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w;
+    }
+  }
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int i = 0; i < VB / 2; ++i) u[i] = 0u;
+  }
+  template <bool PK>
+  __device__ __forceinline__ void fma_into(float (&acc)[VB], float w) const {
+#pragma unroll
+    for (int i = 0; i < VB / 2; ++i) {
+      const float2 f = unpack2<T>(u[i]);
+      if constexpr (PK) {
+        const float b[2] = {f.x, f.y};
+        float a[2] = {acc[2 * i], acc[2 * i + 1]};
+        fma_vec<float, 2>(a, w, b);
+        acc[2 * i] = a[0];
+        acc[2 * i + 1] = a[1];
+      } else {
+        acc[2 * i] = fma(w, f.x, acc[2 * i]);
+        acc[2 * i + 1] = fma(w, f.y, acc[2 * i + 1]);
+      }
+    }
+  }
+};
+template <int VB> struct BVec<__nv_bfloat16, float, VB> : BVec16<__nv_bfloat16, VB> {};
+template <int VB> struct BVec<__half, float, VB> : BVec16<__half, VB> {};
+template <> struct BVec<__nv_bfloat16, float, 1> {
+  float v[1];
+  __device__ __forceinline__ void load(const __nv_bfloat16 *p) { v[0] = __bfloat162float(p[0]); }
+  __device__ __forceinline__ void zero() { v[0] = 0.f; }
+  template <bool PK> __device__ __forceinline__ void fma_into(float (&acc)[1], float w) const {
+    acc[0] = fma(w, v[0], acc[0]);
+  }
+};
+template <> struct BVec<__half, float, 1> {
+  float v[1];
+  __device__ __forceinline__ void load(const __half *p) { v[0] = __half2float(p[0]); }
+  __device__ __forceinline__ void zero() { v[0] = 0.f; }
+  template <bool PK> __device__ __forceinline__ void fma_into(float (&acc)[1], float w) const {
+    acc[0] = fma(w, v[0], acc[0]);
+  }
+};
+
 // C += a (vector reduction in L2).  FP32: one 16-byte float4 atomic (sm_90+); FP64: scalar.
 template <class T, class ACC, int VB>
 __device__ __forceinline__ void vatomic_add(T *__restrict__ p, const ACC (&a)[VB]) {
