@@ -341,6 +341,10 @@ def run_fwdbwd(args):
         plan.fused_forward_backward(X, dY, Y, dX, dA)
 
     t_plain = _timed(plain, args.steps, args.warmup)
+    symmetric = plan.is_symmetric()
+    plan.set_symmetry(False)  # general path: Y and dA in one pass, dX over A^T
+    t_fused_general = _timed(fused, args.steps, args.warmup)
+    plan.set_symmetry(True)
     t_fused = _timed(fused, args.steps, args.warmup)
     t_fwd = _timed(lambda: plan.spmm(X, Y), args.steps, args.warmup)
     t_bwd = _timed(lambda: plan.spmm_t(dY, dX), args.steps, args.warmup)
@@ -353,8 +357,13 @@ def run_fwdbwd(args):
         "config": {"workload": args.workload, "nodes": M, "nnz": nnz, "N": N,
                    "graph": f"R-MAT scale {wl['scale']} symmetrised, no self loops, values 1/sqrt(d_i d_j)"},
         "ratio_fused_vs_plain": t_plain / t_fused,
-        "ms": {"plain_fwd_bwd": t_plain, "fused_fwd_bwd": t_fused, "spmm": t_fwd, "spmm_transposed": t_bwd,
-               "sddmm": t_sddmm},
+        "ratio_fused_general_vs_plain": t_plain / t_fused_general,
+        "symmetric": symmetric,
+        "ms": {"plain_fwd_bwd": t_plain, "fused_fwd_bwd": t_fused, "fused_fwd_bwd_general": t_fused_general,
+               "spmm": t_fwd, "spmm_transposed": t_bwd, "sddmm": t_sddmm},
+        "paths": {"plain": "swift_spmm + swift_spmm_transposed + swift_sddmm, each its own pass",
+                  "fused": "one pass over A for Y, dX (A symmetric: dX = A dY) and dA",
+                  "fused_general": "one pass over A for Y and dA, one over A^T for dX"},
     }
     _single_gpu_line(args, out)
 

@@ -222,9 +222,18 @@ swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const
                          int64_t ldu, const void *V, int64_t ldv, void *out,
                          swift_stream_t stream);
 
+/* Whether A equals its transpose, values included (square plans; computed once on the GPU
+ * and cached; synchronises `stream` the first time).  No counterpart in the reference. */
+swift_status swift_plan_is_symmetric(swift_plan *plan, int *symmetric, swift_stream_t stream);
+/* use = 0 keeps swift_fused_forward_backward on the general path (one pass for Y and dA, one
+ * over A^T for dX) even for a symmetric A; 1 (default) lets it use the symmetry. */
+swift_status swift_plan_set_symmetry(swift_plan *plan, int use);
+
 /* One pass over A in row order for Y = A X and dA_vals = SDDMM(dY, X) (X read once per
- * nonzero for both), then dX = A^T dY over the transposed layout.  Any output pointer may be
- * NULL to skip that product.  Row-major, F32 or F64. */
+ * nonzero for both), then dX = A^T dY over the transposed layout.  When A == A^T with equal
+ * values (checked once per plan, see swift_plan_is_symmetric), dX = A dY joins the same pass
+ * and the transposed layout is not used.  Any output pointer may be NULL to skip that
+ * product.  Row-major, F32 or F64. */
 swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_dtype dtype,
                                           const void *X, int64_t ldx, const void *dY,
                                           int64_t lddy, void *Y, int64_t ldy, void *dX,

@@ -318,7 +318,23 @@ swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const
     SW_CHECK_CUDA(cudaMemsetAsync(out, 0, p.vsz * (size_t)p.nnz, st));
     return SWIFT_OK;
   }
+  const swift_status rc = run_bwd_merge(p, N, dtype, V, ldv, U, ldu, nullptr, 0, nullptr, 0, out, st);
+  if (rc != SWIFT_ERR_UNSUPPORTED) return rc;
   return run_sddmm(p, N, dtype, U, ldu, V, ldv, out, st);
+}
+
+swift_status swift_plan_set_symmetry(swift_plan *plan, int use) {
+  if (!plan || (use != 0 && use != 1)) return SWIFT_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> g(plan->p.mu);
+  plan->p.use_symmetry = use;
+  return SWIFT_OK;
+}
+
+swift_status swift_plan_is_symmetric(swift_plan *plan, int *symmetric, swift_stream_t stream) {
+  if (!plan || !symmetric) return SWIFT_ERR_INVALID_ARG;
+  SW_TRY(check_symmetric(plan->p, S(stream)));
+  *symmetric = plan->p.symmetric;
+  return SWIFT_OK;
 }
 
 swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_dtype dtype,
@@ -332,8 +348,19 @@ swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_d
   SW_TRY(check_dense(plan, N, dtype, X, ldx, SWIFT_ROW_MAJOR, p.K, dY, lddy, SWIFT_ROW_MAJOR, p.M));
   cudaStream_t st = S(stream);
   if (N == 0) return SWIFT_OK;
+  if (Y && dA && dX && p.use_symmetry) {
+    // A == A^T with equal values: dX = A dY joins the same pass over A
+    SW_TRY(check_symmetric(p, st));
+    if (p.symmetric == 1) {
+      const swift_status rc = run_bwd_merge(p, N, dtype, X, ldx, dY, lddy, Y, ldy, dX, lddx, dA, st);
+      if (rc != SWIFT_ERR_UNSUPPORTED) return rc;
+    }
+  }
   if (Y || dA) {
-    if (Y && dA) SW_TRY(run_fused_fwd_sddmm(p, N, dtype, X, ldx, dY, lddy, Y, ldy, dA, st));
+    swift_status rc = SWIFT_ERR_UNSUPPORTED;
+    if (Y && dA) rc = run_bwd_merge(p, N, dtype, X, ldx, dY, lddy, Y, ldy, nullptr, 0, dA, st);
+    if (rc != SWIFT_ERR_UNSUPPORTED) SW_TRY(rc);
+    else if (Y && dA) SW_TRY(run_fused_fwd_sddmm(p, N, dtype, X, ldx, dY, lddy, Y, ldy, dA, st));
     else if (Y) {
       DenseArgs d;
       d.N = N; d.dtype = dtype; d.B = X; d.ldb = ldx; d.C = Y; d.ldc = ldy;

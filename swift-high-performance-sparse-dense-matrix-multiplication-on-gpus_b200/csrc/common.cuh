@@ -130,7 +130,7 @@ struct RowLayout {
   DevBuf task_hdr;                    // [ntasks] int4 packing of the three arrays above
   DevBuf eidx;                        // [nnz] gather indices, bit 31 set on each row's first
   DevBuf split_row, split_first, split_last, split_cnt;  // [nsplit]
-  DevBuf mscratch;                    // [2*ntasks][N] partial rows
+  DevBuf mscratch;                    // [2*ntasks][N] partial rows ([2*ntasks][2N] for [Y | dX])
 };
 
 // Parameters of the merge-path row engine (autotuned per (N, dtype); overridable).
@@ -188,6 +188,10 @@ struct Plan {
   std::map<std::pair<int, int>, MergeOpts> tuned_merge;
   bool merge_override = false;
   MergeOpts merge_opts;  // used when set explicitly, and as the default otherwise
+  // A == A^T including values (square plans): -1 not yet checked, 0 no, 1 yes; the fused
+  // backward then computes dX = A dY in the same pass.  use_symmetry = 0 disables that.
+  int symmetric = -1;
+  int use_symmetry = 1;
   std::mutex mu;  // guards lazily built layouts and scratch growth
 };
 
@@ -250,6 +254,14 @@ swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &a, cudaStream_t
 swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpts &o,
                        cudaStream_t st);
 swift_status build_merge_tasks(RowLayout &L, int U, cudaStream_t st);
+// One merge-path pass over A for any of Y = A X, dA = SDDMM(dY, X) and (A symmetric)
+// dX = A dY; dtype must equal the plan's value type.  SWIFT_ERR_UNSUPPORTED when the shape
+// is not covered (the caller then uses the piece-based kernels).
+swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_t ldx,
+                           const void *dY, int64_t lddy, void *Y, int64_t ldy, void *dX,
+                           int64_t lddx, void *dA, cudaStream_t st);
+// Checks (once) whether A == A^T with equal values; result cached in p.symmetric.
+swift_status check_symmetric(Plan &p, cudaStream_t st);
 swift_status run_f64_reference(const Plan &p, int N, const double *B, int64_t ldb, double *C,
                                int64_t ldc, cudaStream_t st);
 swift_status run_sddmm(Plan &p, int N, swift_dtype dt, const void *U, int64_t ldu,

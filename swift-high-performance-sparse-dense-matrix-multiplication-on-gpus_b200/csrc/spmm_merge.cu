@@ -391,6 +391,239 @@ __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a
   flag_walk<T, TA, ACC, VB, SG>(a, t, sl, sgmask, stage_all[(threadIdx.x >> 5) * G + sg]);
 }
 
+// ---------------------------------------------------------------- backward walks
+// One pass over A in row order for any of: Y = A X (DOY); dA_e = dY[row_e] . X[col_e] (DODA);
+// and, for A == A^T with equal values, dX = A^T dY = A dY (DODX: dY rows are gathered like
+// X rows).  A gathered X row serves both Y and dA; the current row's dY slice stays in
+// registers.  dA is reduced across the sub-warp four nonzeros at a time (5 shuffles per 4).
+struct BwdArgs {
+  MergeArgs m;     // X in m.B / m.ldb, Y in m.C / m.ldc, Y partials in m.scratch
+  const void *dY;  // M x N: per-row operand of dA, gathered operand of dX
+  int64_t lddy;
+  void *dX;
+  int64_t lddx;
+  void *dA;        // nnz values in CSR order
+};
+
+// Sum over the SG lanes of a sub-warp of four per-lane values; every lane returns the total
+// of value (2 * h1 + h2), h1 = lane bit SG/2, h2 = lane bit SG/4.  Needs SG >= 4.
+template <class T, int SG>
+__device__ __forceinline__ T reduce4(T p0, T p1, T p2, T p3, int sl, unsigned m) {
+  const bool h1 = sl & (SG / 2), h2 = sl & (SG / 4);
+  T k0 = h1 ? p2 : p0, k1 = h1 ? p3 : p1;
+  const T s0 = h1 ? p0 : p2, s1 = h1 ? p1 : p3;
+  k0 += __shfl_xor_sync(m, s0, SG / 2, SG);
+  k1 += __shfl_xor_sync(m, s1, SG / 2, SG);
+  T k = h2 ? k1 : k0;
+  const T s = h2 ? k0 : k1;
+  k += __shfl_xor_sync(m, s, SG / 4, SG);
+#pragma unroll
+  for (int o = SG / 8; o >= 1; o >>= 1) k += __shfl_xor_sync(m, k, o, SG);
+  return k;
+}
+
+template <class T, int SG>
+__device__ __forceinline__ T reduce1(T v, unsigned m) {
+#pragma unroll
+  for (int o = SG / 2; o >= 1; o >>= 1) v += __shfl_xor_sync(m, v, o, SG);
+  return v;
+}
+
+// Last-arriving task of split row s adds the partials in task order.  Scratch rows hold
+// W = N values, or 2N when [Y | dX] are produced together (lanes of the second half of the
+// sub-warp own dX).
+template <class T, int VB, int SG, bool DODX>
+__device__ __forceinline__ void arrive_bwd(const BwdArgs &ba, int s, int sl, unsigned sgmask) {
+  const MergeArgs &a = ba.m;
+  __threadfence();
+  __syncwarp(sgmask);
+  int old = 0;
+  if (sl == 0) old = atomicAdd(a.split_cnt + s, 1);
+  old = __shfl_sync(sgmask, old, 0, SG);
+  const int ta = a.split_first[s], tb = a.split_last[s];
+  if (old != tb - ta) return;
+  __threadfence();
+  constexpr int H = DODX ? SG / 2 : SG;
+  const int row = a.split_row[s];
+  const int role = DODX ? sl / H : 0, lsl = sl % H;
+  const int64_t W = DODX ? 2 * (int64_t)a.N : a.N;
+  if (lsl * VB < a.N) {
+    T y[VB];
+#pragma unroll
+    for (int e = 0; e < VB; ++e) y[e] = T(0);
+    const T *s1 = static_cast<const T *>(a.scratch);
+    for (int t = ta; t <= tb; ++t) {
+      const int64_t off = (int64_t)(t == ta ? 2 * t + 1 : 2 * t) * W + role * a.N + lsl * VB;
+#pragma unroll
+      for (int e = 0; e < VB; ++e) y[e] += __ldcg(s1 + off + e);
+    }
+    T *dst = role ? static_cast<T *>(ba.dX) + (int64_t)row * ba.lddx : static_cast<T *>(a.C) + (int64_t)row * a.ldc;
+    vstore<T, T, VB>(dst + lsl * VB, y);
+  }
+  __syncwarp(sgmask);
+  if (sl == 0) a.split_cnt[s] = 0;
+}
+
+// With DODX the sub-warp splits in two halves: lanes [0, SG/2) gather X rows and accumulate
+// Y, lanes [SG/2, SG) gather dY rows and accumulate dX -- the product with [X | dY] of twice
+// the width -- so each lane keeps one gathered vector per nonzero.
+template <class T, int VB, int SG, bool DOY, bool DODA, bool DODX, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) {
+  static_assert(SG >= 4, "the four-value reduction needs sub-warps of 4 or more lanes");
+  constexpr int G = 32 / SG;
+  constexpr int UNR = 4;
+  constexpr int H = DODX ? SG / 2 : SG;
+  constexpr bool F64 = sizeof(T) == 8;
+  __shared__ int2 stage_all[8 * G][32];
+  __shared__ T vstage_all[F64 ? 8 * G : 1][32];
+  const MergeArgs &a = ba.m;
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  int2 *stage = stage_all[(threadIdx.x >> 5) * G + sg];
+  T *vstage = vstage_all[F64 ? (threadIdx.x >> 5) * G + sg : 0];
+  const int role = DODX ? sl / H : 0, lsl = sl % H;
+  const int64_t W = DODX ? 2 * (int64_t)a.N : a.N;
+  const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
+  const int64_t d0 = (int64_t)t * a.U;
+  const int p = (int)(d0 - hdr.x);
+  const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
+  const bool inb = lsl * VB < a.N;
+  T acc[VB], urow[VB];
+#pragma unroll
+  for (int e = 0; e < VB; ++e) acc[e] = urow[e] = T(0);
+  const T *dYp = static_cast<const T *>(ba.dY);
+  auto load_u = [&](int row) {
+    if (DODA) {
+      if (role == 0 && inb && row < a.rows) vload<T, T, VB>(dYp + (int64_t)row * ba.lddy + lsl * VB, urow);
+      else {
+#pragma unroll
+        for (int e = 0; e < VB; ++e) urow[e] = T(0);
+      }
+    }
+  };
+  int cur = hdr.x, rbase = cur;
+  int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+  int pe = __shfl_sync(sgmask, myend, 0, SG);
+  load_u(cur);
+  auto finish_and_advance = [&]() {
+    if (DOY || DODX) {
+      if (cur == hdr.x && hdr.z >= 0) {
+        if (inb) {
+          T *dst = static_cast<T *>(a.scratch) + (int64_t)(2 * t) * W + role * a.N + lsl * VB;
+#pragma unroll
+          for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+        }
+      } else if (inb) {
+        T *dst = role ? static_cast<T *>(ba.dX) + (int64_t)cur * ba.lddx : static_cast<T *>(a.C) + (int64_t)cur * a.ldc;
+        vstore<T, T, VB>(dst + lsl * VB, acc);
+      }
+#pragma unroll
+      for (int e = 0; e < VB; ++e) acc[e] = T(0);
+    }
+    ++cur;
+    if (cur - rbase >= SG) {
+      rbase = cur;
+      myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+    }
+    pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
+    load_u(cur);
+  };
+  const char *Gl = role ? reinterpret_cast<const char *>(dYp + lsl * VB)
+                        : reinterpret_cast<const char *>(static_cast<const T *>(a.B) + lsl * VB);
+  // 32 x 32 -> 64-bit row offsets (the launch guarantees ld * sizeof(T) < 2^32)
+  const uint32_t g_ld = (uint32_t)((role ? ba.lddy : a.ldb) * (int64_t)sizeof(T));
+  constexpr unsigned LOW = SG == 32 ? 0xffffffffu : ((1u << SG) - 1u);
+  const T *val = static_cast<const T *>(a.val);
+  T *dA = static_cast<T *>(ba.dA);
+  for (int q0 = p; q0 < pn; q0 += 32) {
+    const int m = min(32, pn - q0);
+    unsigned rs = 0;
+    __syncwarp(sgmask);
+#pragma unroll
+    for (int i = 0; i < 32 / SG; ++i) {
+      const int j = sl + i * SG;
+      int2 e = make_int2(0, 0);
+      if (j < m) {
+        e.x = __ldcs(a.idx + q0 + j);
+        if (DOY || DODX) {
+          if (F64) vstage[j] = __ldcs(val + q0 + j);
+          else e.y = __float_as_int((float)__ldcs(val + q0 + j));
+        }
+      }
+      rs |= ((__ballot_sync(sgmask, e.x < 0) >> (sg * SG)) & LOW) << (i * SG);
+      e.x &= 0x7fffffff;
+      stage[j] = e;
+    }
+    __syncwarp(sgmask);
+    for (int k = 0; k < m; k += UNR) {
+      BVec<T, T, VB> x[UNR];
+      T part[UNR];
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        const bool ok = k + u < m;
+        const uint32_t c = ok ? (uint32_t)stage[k + u].x : 0u;
+        if (inb && ok) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)c * g_ld));
+        else x[u].zero();
+        part[u] = T(0);
+      }
+      const bool starts = (rs >> k) & 0xFu;
+#pragma unroll
+      for (int u = 0; u < UNR; ++u) {
+        if (k + u >= m) break;
+        if (starts) {
+          while (q0 + k + u == pe) finish_and_advance();
+        }
+        if (DOY || DODX) {
+          const T w = F64 ? vstage[k + u] : (T)__int_as_float(stage[k + u].y);
+          x[u].template fma_into<true>(acc, w);
+        }
+        if (DODA) {
+          T d = T(0);
+#pragma unroll
+          for (int e = 0; e < VB; ++e) d = fma(urow[e], x[u].v[e], d);
+          part[u] = d;
+        }
+      }
+      if (DODA) {
+        const T r = reduce4<T, SG>(part[0], part[1], part[2], part[3], sl, sgmask);
+        const int idx = ((sl & (SG / 2)) ? 2 : 0) + ((sl & (SG / 4)) ? 1 : 0);
+        if ((sl & (SG / 4 - 1)) == 0 && k + idx < m) dA[q0 + k + idx] = r;
+      }
+    }
+  }
+  while (cur < hdr.y) finish_and_advance();
+  if (DOY || DODX) {
+    if (hdr.w >= 0 && inb) {
+      T *dst = static_cast<T *>(a.scratch) + (int64_t)((hdr.z >= 0 && hdr.x == hdr.y) ? 2 * t : 2 * t + 1) * W +
+               role * a.N + lsl * VB;
+#pragma unroll
+      for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
+    }
+    if (hdr.z >= 0 && hdr.x < hdr.y) arrive_bwd<T, VB, SG, DODX>(ba, hdr.z, sl, sgmask);
+    if (hdr.w >= 0) arrive_bwd<T, VB, SG, DODX>(ba, hdr.w, sl, sgmask);
+  }
+}
+
+template <class T>
+__global__ void sym_check_kernel(int M, const int *__restrict__ rowptr, const int *__restrict__ colidx,
+                                 const T *__restrict__ val, const int *__restrict__ invperm,
+                                 const int *__restrict__ sptr, const int *__restrict__ srow,
+                                 const T *__restrict__ sval, int *__restrict__ bad) {
+  const int warps = (gridDim.x * blockDim.x) >> 5, lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < M; r += warps) {
+    const int i = invperm[r];
+    const int a0 = rowptr[r], len = rowptr[r + 1] - a0, b0 = sptr[i];
+    if (len != sptr[i + 1] - b0) {
+      if (lane == 0) *bad = 1;
+      continue;
+    }
+    for (int j = lane; j < len; j += 32)
+      if (colidx[a0 + j] != srow[b0 + j] || !(val[a0 + j] == sval[b0 + j])) *bad = 1;
+  }
+}
+
 // Batched products in one persistent launch: matrix i owns warp items
 // [item_off[i], item_off[i+1]), each item G_i = 32 / SG_i consecutive tasks of its plan; the
 // sub-warp width follows that matrix's N (16-byte vectors for N <= 128, or scalars for
@@ -610,18 +843,20 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
 #define SW_MCASE_FLAG(VB_, SG_)                                                                 \
   if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_)                                   \
     return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T))>(a, eidx, st);
-  if (sizeof(TA) == 4 && (kernel == 2 || (kernel == 0 && unr <= 4))) {
-    SW_MCASE_FLAG(W, 2)
-    SW_MCASE_FLAG(W, 4)
-    SW_MCASE_FLAG(W, 8)
-    SW_MCASE_FLAG(W, 16)
-    SW_MCASE_FLAG(W, 32)
-    SW_MCASE_FLAG(V, 2)
-    SW_MCASE_FLAG(V, 4)
-    SW_MCASE_FLAG(V, 8)
-    SW_MCASE_FLAG(V, 16)
-    SW_MCASE_FLAG(V, 32)
-    SW_MCASE_FLAG(1, 32)
+  if constexpr (sizeof(TA) == 4) {
+    if (kernel == 2 || (kernel == 0 && unr <= 4)) {
+      SW_MCASE_FLAG(W, 2)
+      SW_MCASE_FLAG(W, 4)
+      SW_MCASE_FLAG(W, 8)
+      SW_MCASE_FLAG(W, 16)
+      SW_MCASE_FLAG(W, 32)
+      SW_MCASE_FLAG(V, 2)
+      SW_MCASE_FLAG(V, 4)
+      SW_MCASE_FLAG(V, 8)
+      SW_MCASE_FLAG(V, 16)
+      SW_MCASE_FLAG(V, 32)
+      SW_MCASE_FLAG(1, 32)
+    }
   }
 #undef SW_MCASE_FLAG
 #define SW_MCASE(VB_, SG_, VPL_)                                                              \
@@ -722,6 +957,125 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
     default: return SWIFT_ERR_UNSUPPORTED;
   }
 #undef SW_MDISPATCH
+}
+
+namespace {
+
+constexpr int bwd_minb(int VB, int AB, bool DODX) {
+  const int regs = 32 + (VB * AB / 4) * 6 + 4 * AB / 4 + (DODX ? 4 : 0);
+  const int b = 65536 / (256 * regs);
+  return b < 1 ? 1 : (b > 8 ? 8 : b);
+}
+
+template <class T, int VB, int SG, bool DOY, bool DODA, bool DODX>
+swift_status launch_bwd(const BwdArgs &ba, cudaStream_t st) {
+  constexpr int G = 32 / SG;
+  const int64_t warps = ((int64_t)ba.m.ntasks + G - 1) / G;
+  if (warps == 0) return SWIFT_OK;
+  merge_bwd_kernel<T, VB, SG, DOY, DODA, DODX, bwd_minb(VB, (int)sizeof(T), DODX)>
+      <<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(ba);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+template <class T, int VB, bool DOY, bool DODA, bool DODX>
+swift_status bwd_by_sg(const BwdArgs &ba, int SG, cudaStream_t st) {
+  switch (SG) {
+    case 4: return launch_bwd<T, VB, 4, DOY, DODA, DODX>(ba, st);
+    case 8: return launch_bwd<T, VB, 8, DOY, DODA, DODX>(ba, st);
+    case 16: return launch_bwd<T, VB, 16, DOY, DODA, DODX>(ba, st);
+    case 32: return launch_bwd<T, VB, 32, DOY, DODA, DODX>(ba, st);
+  }
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
+template <class T, bool DOY, bool DODA, bool DODX>
+swift_status bwd_by_vb(const BwdArgs &ba, int VB, int SG, cudaStream_t st) {
+  constexpr int V = VecWidth<T>::value;
+  if (VB == V) return bwd_by_sg<T, V, DOY, DODA, DODX>(ba, SG, st);
+  if (VB == 1) return bwd_by_sg<T, 1, DOY, DODA, DODX>(ba, SG, st);
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
+template <class T>
+swift_status bwd_dispatch(const BwdArgs &ba, int VB, int SG, bool y, bool da, bool dx, cudaStream_t st) {
+  if (y && da && dx) return bwd_by_vb<T, true, true, true>(ba, VB, SG, st);
+  if (y && da) return bwd_by_vb<T, true, true, false>(ba, VB, SG, st);
+  if (da && !y && !dx) return bwd_by_vb<T, false, true, false>(ba, VB, SG, st);
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+swift_status check_symmetric(Plan &p, cudaStream_t st) {
+  if (p.symmetric >= 0) return SWIFT_OK;
+  if (!p.has_csr || p.M != p.K) {
+    p.symmetric = 0;
+    return SWIFT_OK;
+  }
+  TmpBuf bad;
+  SW_TRY(bad.alloc(sizeof(int), st));
+  SW_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+  if (p.M > 0) {
+    const int blocks = (int)std::min<int64_t>(((int64_t)p.M * 32 + 255) / 256, 148 * 32);
+    if (p.val_type == SWIFT_F64)
+      sym_check_kernel<double><<<blocks, 256, 0, st>>>(p.M, p.rowptr.as<int>(), p.colidx.as<int>(),
+                                                        p.val.as<double>(), p.invperm.as<int>(), p.sptr.as<int>(),
+                                                        p.srow.as<int>(), p.sval.as<double>(), bad.as<int>());
+    else
+      sym_check_kernel<float><<<blocks, 256, 0, st>>>(p.M, p.rowptr.as<int>(), p.colidx.as<int>(),
+                                                       p.val.as<float>(), p.invperm.as<int>(), p.sptr.as<int>(),
+                                                       p.srow.as<int>(), p.sval.as<float>(), bad.as<int>());
+    SW_CHECK_LAUNCH();
+  }
+  int h = 0;
+  SW_CHECK_CUDA(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  p.symmetric = h ? 0 : 1;
+  return SWIFT_OK;
+}
+
+swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_t ldx,
+                           const void *dY, int64_t lddy, void *Y, int64_t ldy, void *dX,
+                           int64_t lddx, void *dA, cudaStream_t st) {
+  if (!p.has_csr || dt != p.val_type || (dt != SWIFT_F32 && dt != SWIFT_F64)) return SWIFT_ERR_UNSUPPORTED;
+  if (dX && (p.M != p.K || p.symmetric != 1)) return SWIFT_ERR_UNSUPPORTED;
+  if (N <= 0 || p.M == 0) return SWIFT_ERR_UNSUPPORTED;
+  const size_t esz = dt == SWIFT_F64 ? 8 : 4;
+  if (ldx * (int64_t)esz >= (int64_t(1) << 32) || lddy * (int64_t)esz >= (int64_t(1) << 32))
+    return SWIFT_ERR_UNSUPPORTED;
+  const int V = (int)(16 / esz);
+  auto al = [&](const void *q, int64_t ld) {
+    return !q || (((uintptr_t)q % 16 == 0) && ((ld * (int64_t)esz) % 16 == 0));
+  };
+  int VB = 1;
+  if (N % V == 0 && N / V <= 32 && al(X, ldx) && al(dY, lddy) && al(Y, ldy) && al(dX, lddx)) VB = V;
+  const int lanes = ((N + VB - 1) / VB) * (dX ? 2 : 1);
+  if (lanes > 32) return SWIFT_ERR_UNSUPPORTED;
+  int SG = 4;
+  while (SG < lanes) SG <<= 1;
+  RowLayout &L = p.fwd;
+  {
+    std::lock_guard<std::mutex> g(p.mu);
+    SW_TRY(build_merge_tasks(L, L.merge_built ? L.merge_U : 512, st));
+    const size_t need = (size_t)2 * L.ntasks * (size_t)N * (dX ? 2 : 1) * esz;
+    if ((Y || dX) && need > L.mscratch.bytes) SW_TRY(L.mscratch.alloc(need));
+  }
+  BwdArgs ba{};
+  MergeArgs &a = ba.m;
+  a.rows = L.rows; a.N = N; a.U = L.merge_U; a.ntasks = L.ntasks;
+  a.total = (int64_t)L.nnz + L.rows;
+  a.ptr = L.ptr; a.idx = L.eidx.as<int>(); a.val = L.val; a.out_row = nullptr;
+  a.B = X; a.ldb = ldx; a.C = Y; a.ldc = ldy;
+  a.task_row = L.task_row.as<int>(); a.head_split = L.head_split.as<int>(); a.tail_split = L.tail_split.as<int>();
+  a.task_hdr = L.task_hdr.as<int>();
+  a.split_row = L.split_row.as<int>(); a.split_first = L.split_first.as<int>();
+  a.split_last = L.split_last.as<int>(); a.split_cnt = L.split_cnt.as<int>();
+  a.scratch = L.mscratch.p;
+  ba.dY = dY; ba.lddy = lddy; ba.dX = dX; ba.lddx = lddx; ba.dA = dA;
+  const bool y = Y != nullptr, da = dA != nullptr, dx = dX != nullptr;
+  return dt == SWIFT_F64 ? bwd_dispatch<double>(ba, VB, SG, y, da, dx, st)
+                         : bwd_dispatch<float>(ba, VB, SG, y, da, dx, st);
 }
 
 size_t merge_args_size() { return sizeof(MergeArgs); }

@@ -124,6 +124,8 @@ _SIGS = [
     ("swift_plan_destroy", C.c_int, [_P]),
     ("swift_plan_get_stats", C.c_int, [_P, C.POINTER(swift_plan_stats)]),
     ("swift_plan_set_values", C.c_int, [_P, _P, C.c_int, _P]),
+    ("swift_plan_is_symmetric", C.c_int, [_P, C.POINTER(C.c_int), _P]),
+    ("swift_plan_set_symmetry", C.c_int, [_P, C.c_int]),
     ("swift_plan_export_f32", C.c_int, [_P, C.POINTER(swift_slide_matrix_f32), C.c_int, C.POINTER(C.c_float)]),
     ("swift_plan_export_f64", C.c_int, [_P, C.POINTER(swift_slide_matrix_f64), C.c_int, C.POINTER(C.c_float)]),
     ("swift_slide_free_f32", None, [C.POINTER(swift_slide_matrix_f32)]),

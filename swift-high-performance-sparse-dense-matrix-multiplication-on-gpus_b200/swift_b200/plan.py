@@ -127,6 +127,18 @@ class Plan:
         d["fmt_count"] = list(s.fmt_count)
         return d
 
+    def is_symmetric(self, stream=None) -> bool:
+        """A == A^T with equal values (checked once on the GPU, then cached)."""
+        s = C.c_int(0)
+        capi.check(capi.lib().swift_plan_is_symmetric(self._h, C.byref(s), _stream_ptr(stream)),
+                   "swift_plan_is_symmetric")
+        return s.value == 1
+
+    def set_symmetry(self, use: bool):
+        """Whether fused_forward_backward may compute dX = A dY in its first pass when A is
+        symmetric (default True)."""
+        capi.check(capi.lib().swift_plan_set_symmetry(self._h, int(bool(use))), "swift_plan_set_symmetry")
+
     def set_values(self, val, stream=None):
         """New values for the fixed pattern (CSR order; numpy or a CUDA tensor of the plan's
         value type)."""
