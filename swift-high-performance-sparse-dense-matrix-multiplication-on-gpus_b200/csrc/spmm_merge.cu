@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
 // with one broadcast load per nonzero; full chunks run fully unrolled.
 // One task of the flagged walk by one sub-warp (sl = lane within the sub-warp, stage = its
 // 32-entry staging buffer).
-template <class T, class TA, class ACC, int VB, int SG>
+template <class T, class TA, class ACC, int VB, int SG, bool FULL = false>
 __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, unsigned sgmask,
                                           int2 *stage) {
   constexpr int UNR = 4;
@@ -292,7 +292,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
   const int64_t d0 = (int64_t)t * a.U;
   const int p = (int)(d0 - hdr.x);
   const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
-  const bool inb = sl * VB < a.N;
+  const bool inb = FULL || sl * VB < a.N;
   ACC acc[VB];
 #pragma unroll
   for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
@@ -321,7 +321,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
   };
   auto accumulate = [&](float wf, const BVec<T, ACC, VB> &b) { b.template fma_into<true>(acc, (ACC)wf); };
   const char *Bl = reinterpret_cast<const char *>(static_cast<const T *>(a.B) + sl * VB);
-  const int64_t ldb_bytes = a.ldb * (int64_t)sizeof(T);
+  const uint32_t ldb_bytes = (uint32_t)(a.ldb * (int64_t)sizeof(T));  // < 2^32 (checked at launch)
   const TA *val = static_cast<const TA *>(a.val);
   for (int q0 = p; q0 < pn; q0 += 32) {
     const int m = min(32, pn - q0);
@@ -345,7 +345,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
         for (int u = 0; u < UNR; ++u) {
           const int c = stage[k + u].x;
           flags |= c;
-          if (inb) b[u].load(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes));
+          if (inb) b[u].load(reinterpret_cast<const T *>(Bl + (uint64_t)(uint32_t)(c & 0x7fffffff) * ldb_bytes));
           else b[u].zero();
         }
         if (flags < 0) {
@@ -363,7 +363,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
       for (int k = 0; k < m; ++k) {
         const int c = stage[k].x;
         BVec<T, ACC, VB> b;
-        if (inb) b.load(reinterpret_cast<const T *>(Bl + (int64_t)(c & 0x7fffffff) * ldb_bytes));
+        if (inb) b.load(reinterpret_cast<const T *>(Bl + (uint64_t)(uint32_t)(c & 0x7fffffff) * ldb_bytes));
         else b.zero();
         while (q0 + k == pe) finish_and_advance();
         accumulate(__int_as_float(stage[k].y), b);
@@ -380,7 +380,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
   if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1>(a, hdr.w, sl, sgmask);
 }
 
-template <class T, class TA, class ACC, int VB, int SG, int MINB>
+template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL>
 __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
   constexpr int G = 32 / SG;
   __shared__ int2 stage_all[8 * G][32];
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a
   const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
   const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
   if (t >= a.ntasks) return;
-  flag_walk<T, TA, ACC, VB, SG>(a, t, sl, sgmask, stage_all[(threadIdx.x >> 5) * G + sg]);
+  flag_walk<T, TA, ACC, VB, SG, FULL>(a, t, sl, sgmask, stage_all[(threadIdx.x >> 5) * G + sg]);
 }
 
 // ---------------------------------------------------------------- backward walks
@@ -647,18 +647,21 @@ __global__ void __launch_bounds__(256, 4) merge_batch_kernel(const MergeArgs *__
     const MergeArgs &a = args[lo];
     const int item = (int)(w - __ldg(item_off + lo));
     switch (__ldg(shape + lo)) {
-#define SW_BATCH_SHAPE(CODE, VB_, SG_)                                                          \
+#define SW_BATCH_SHAPE(CODE, VB_, SG_, FULL_)                                                          \
   case CODE: {                                                                                  \
     const int sg = lane / SG_, sl = lane % SG_;                                                 \
     const unsigned m = SG_ == 32 ? 0xffffffffu : (((1u << SG_) - 1u) << (sg * SG_));            \
     const int t = item * (32 / SG_) + sg;                                                       \
-    if (t < a.ntasks) flag_walk<float, float, float, VB_, SG_>(a, t, sl, m, stage_all[warp * 4 + sg]); \
+    if (t < a.ntasks) flag_walk<float, float, float, VB_, SG_, FULL_>(a, t, sl, m, stage_all[warp * 4 + sg]); \
     break;                                                                                      \
   }
-      SW_BATCH_SHAPE(0, 4, 8)
-      SW_BATCH_SHAPE(1, 4, 16)
-      SW_BATCH_SHAPE(2, 4, 32)
-      SW_BATCH_SHAPE(3, 1, 32)
+      SW_BATCH_SHAPE(0, 4, 8, false)
+      SW_BATCH_SHAPE(1, 4, 16, false)
+      SW_BATCH_SHAPE(2, 4, 32, false)
+      SW_BATCH_SHAPE(3, 1, 32, false)
+      SW_BATCH_SHAPE(4, 4, 8, true)
+      SW_BATCH_SHAPE(5, 4, 16, true)
+      SW_BATCH_SHAPE(6, 4, 32, true)
 #undef SW_BATCH_SHAPE
       default: break;
     }
@@ -810,13 +813,13 @@ constexpr int flag_minb(int VB, int AB, int TB) {
   return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-template <class T, class TA, class ACC, int VB, int SG, int MINB>
+template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL>
 swift_status launch_flag(MergeArgs a, const int *eidx, cudaStream_t st) {
   constexpr int G = 32 / SG;
   const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
   if (warps == 0) return SWIFT_OK;
   a.idx = eidx;
-  merge_flag_kernel<T, TA, ACC, VB, SG, MINB><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
+  merge_flag_kernel<T, TA, ACC, VB, SG, MINB, FULL><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
 }
@@ -842,9 +845,11 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   // flagged-index kernel (FP32-valued plans): 4 loads in flight
 #define SW_MCASE_FLAG(VB_, SG_)                                                                 \
   if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_)                                   \
-    return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T))>(a, eidx, st);
+  { if (a.N == SG_ * VB_) return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), true>(a, eidx, st); \
+    return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), false>(a, eidx, st); }
   if constexpr (sizeof(TA) == 4) {
-    if (kernel == 2 || (kernel == 0 && unr <= 4)) {
+    if ((kernel == 2 || (kernel == 0 && unr <= 4)) &&
+        a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32)) {
       SW_MCASE_FLAG(W, 2)
       SW_MCASE_FLAG(W, 4)
       SW_MCASE_FLAG(W, 8)
@@ -1090,9 +1095,11 @@ swift_status merge_batch_member(const Plan &p, RowLayout &L, int U, int N, const
   const bool v16 = ((uintptr_t)B % 16 == 0) && ((uintptr_t)C % 16 == 0) && (ldb % 4 == 0) &&
                    (ldc % 4 == 0) && (N % 4 == 0);
   int sh, G;
+  if (ldb * (int64_t)sizeof(float) >= (int64_t(1) << 32)) return SWIFT_ERR_UNSUPPORTED;
   if (v16 && N <= 128) {
     sh = N <= 32 ? 0 : (N <= 64 ? 1 : 2);
     G = sh == 0 ? 4 : (sh == 1 ? 2 : 1);
+    if (N == 32 || N == 64 || N == 128) sh += 4;  // every lane in range: no bounds predicate
   } else if (N <= 32) {
     sh = 3;
     G = 1;
