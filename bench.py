@@ -571,6 +571,19 @@ def run_ours(args):
                  "hbm_frac_of_measured": alg_bytes / (t_ms / 1e3) / 1e9 / peak}
         plan.spmm(B, C)
 
+    # context only: the vendor library's CSR SpMM (torch.sparse -> cuSPARSE) on the same inputs
+    library = None
+    try:
+        A_t = torch.sparse_csr_tensor(torch.from_numpy(rp).cuda().long(), torch.from_numpy(ci).cuda().long(),
+                                      val, size=(M, K))
+        Bl = B if B.dtype == val.dtype else B.to(val.dtype)
+        lib_ms = _timed(lambda: torch.sparse.mm(A_t, Bl), 5, 2)
+        library = {"what": "torch.sparse.mm on a CSR tensor (cuSPARSE SpMM)", "ms_per_step": lib_ms,
+                   "gflops": flops / (lib_ms / 1e3) / 1e9}
+        del A_t
+    except Exception as ex:  # context row only
+        library = {"what": "torch.sparse.mm on a CSR tensor", "error": str(ex)[:200]}
+
     # end to end through the public call: every step copies its B in from pinned host memory
     # and its C out to pinned host memory.  Copies in, products and copies out run on three
     # streams over two device buffer sets, so step i's C leaves while step i+1's B arrives
@@ -671,6 +684,7 @@ def run_ours(args):
         "clocks": clocks,
         "cpu_baseline": cpu,
         "tiled_engine": tiled,
+        "library_context": library,
     }
     print(json.dumps(out), flush=True)
     plan.close()

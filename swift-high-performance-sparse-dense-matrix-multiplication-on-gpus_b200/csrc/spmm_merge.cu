@@ -286,7 +286,8 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
 // 32-entry staging buffer).
 template <class T, class TA, class ACC, int VB, int SG, bool FULL = false>
 __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, unsigned sgmask,
-                                          int2 *stage) {
+                                          int2 *stage, ACC *vstage) {
+  // FP32 values ride in stage[].y; FP64 values are staged in vstage
   constexpr int UNR = 4;
   const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
   const int64_t d0 = (int64_t)t * a.U;
@@ -319,7 +320,11 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
     }
     pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
   };
-  auto accumulate = [&](float wf, const BVec<T, ACC, VB> &b) { b.template fma_into<true>(acc, (ACC)wf); };
+  auto accumulate = [&](ACC w, const BVec<T, ACC, VB> &b) { b.template fma_into<true>(acc, w); };
+  auto value_at = [&](int j) -> ACC {
+    if constexpr (sizeof(TA) == 8) return vstage[j];
+    else return (ACC)__int_as_float(stage[j].y);
+  };
   const char *Bl = reinterpret_cast<const char *>(static_cast<const T *>(a.B) + sl * VB);
   const uint32_t ldb_bytes = (uint32_t)(a.ldb * (int64_t)sizeof(T));  // < 2^32 (checked at launch)
   const TA *val = static_cast<const TA *>(a.val);
@@ -331,7 +336,8 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
       int2 e = make_int2(0, 0);
       if (j < m) {
         e.x = __ldcs(a.idx + q0 + j);
-        e.y = __float_as_int((float)__ldcs(val + q0 + j));
+        if constexpr (sizeof(TA) == 8) vstage[j] = (ACC)__ldcs(val + q0 + j);
+        else e.y = __float_as_int((float)__ldcs(val + q0 + j));
       }
       stage[j] = e;
     }
@@ -352,11 +358,11 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
 #pragma unroll
           for (int u = 0; u < UNR; ++u) {
             while (q0 + k + u == pe) finish_and_advance();
-            accumulate(__int_as_float(stage[k + u].y), b[u]);
+            accumulate(value_at(k + u), b[u]);
           }
         } else {
 #pragma unroll
-          for (int u = 0; u < UNR; ++u) accumulate(__int_as_float(stage[k + u].y), b[u]);
+          for (int u = 0; u < UNR; ++u) accumulate(value_at(k + u), b[u]);
         }
       }
     } else {
@@ -366,7 +372,7 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
         if (inb) b.load(reinterpret_cast<const T *>(Bl + (uint64_t)(uint32_t)(c & 0x7fffffff) * ldb_bytes));
         else b.zero();
         while (q0 + k == pe) finish_and_advance();
-        accumulate(__int_as_float(stage[k].y), b);
+        accumulate(value_at(k), b);
       }
     }
   }
@@ -384,11 +390,13 @@ template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL>
 __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
   constexpr int G = 32 / SG;
   __shared__ int2 stage_all[8 * G][32];
+  __shared__ ACC vstage_all[sizeof(TA) == 8 ? 8 * G : 1][32];
   const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
   const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
   const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
   if (t >= a.ntasks) return;
-  flag_walk<T, TA, ACC, VB, SG, FULL>(a, t, sl, sgmask, stage_all[(threadIdx.x >> 5) * G + sg]);
+  const int w = (threadIdx.x >> 5) * G + sg;
+  flag_walk<T, TA, ACC, VB, SG, FULL>(a, t, sl, sgmask, stage_all[w], vstage_all[sizeof(TA) == 8 ? w : 0]);
 }
 
 // ---------------------------------------------------------------- backward walks
@@ -652,7 +660,7 @@ __global__ void __launch_bounds__(256, 4) merge_batch_kernel(const MergeArgs *__
     const int sg = lane / SG_, sl = lane % SG_;                                                 \
     const unsigned m = SG_ == 32 ? 0xffffffffu : (((1u << SG_) - 1u) << (sg * SG_));            \
     const int t = item * (32 / SG_) + sg;                                                       \
-    if (t < a.ntasks) flag_walk<float, float, float, VB_, SG_, FULL_>(a, t, sl, m, stage_all[warp * 4 + sg]); \
+    if (t < a.ntasks) flag_walk<float, float, float, VB_, SG_, FULL_>(a, t, sl, m, stage_all[warp * 4 + sg], nullptr); \
     break;                                                                                      \
   }
       SW_BATCH_SHAPE(0, 4, 8, false)
@@ -843,11 +851,15 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   constexpr int W = WideWidth<T>::value;
   constexpr int AB = (int)sizeof(ACC);
   // flagged-index kernel (FP32-valued plans): 4 loads in flight
+  // (FP64 values double the staging; 2-lane sub-warps would exceed 48 KB of static shared memory)
 #define SW_MCASE_FLAG(VB_, SG_)                                                                 \
-  if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_)                                   \
-  { if (a.N == SG_ * VB_) return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), true>(a, eidx, st); \
-    return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), false>(a, eidx, st); }
-  if constexpr (sizeof(TA) == 4) {
+  if constexpr (sizeof(TA) == 4 || SG_ >= 4) {                                                  \
+    if (VB == VB_ && SG == SG_ && VPL == 1 && a.N <= SG_ * VB_) {                               \
+      if (a.N == SG_ * VB_) return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), true>(a, eidx, st); \
+      return launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), false>(a, eidx, st); \
+    }                                                                                           \
+  }
+  {
     if ((kernel == 2 || (kernel == 0 && unr <= 4)) &&
         a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32)) {
       SW_MCASE_FLAG(W, 2)
