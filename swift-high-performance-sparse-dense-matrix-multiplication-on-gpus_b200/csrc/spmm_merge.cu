@@ -215,8 +215,12 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
   ACC acc[VB];
 #pragma unroll
   for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+  // row ends of the next SG rows, one per lane; the block after it is fetched one block ahead
+  // so that crossing into it never waits on memory
   int cur = hdr.x, rbase = cur;
-  int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+  auto rowend = [&](int r) { return r <= a.rows ? __ldg(a.ptr + r) : 0x7fffffff; };
+  int myend = rowend(rbase + 1 + sl);
+  int myend2 = rowend(rbase + SG + 1 + sl);
   int pe = __shfl_sync(sgmask, myend, 0, SG);
   auto finish_and_advance = [&]() {
     if (cur == hdr.x && hdr.z >= 0) {
@@ -233,8 +237,9 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
     for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
     ++cur;
     if (cur - rbase >= SG) {
-      rbase = cur;
-      myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+      rbase += SG;
+      myend = myend2;
+      myend2 = rowend(rbase + SG + 1 + sl);
     }
     pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
   };
@@ -297,8 +302,12 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
   ACC acc[VB];
 #pragma unroll
   for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+  // row ends of the next SG rows, one per lane; the block after it is fetched one block ahead
+  // so that crossing into it never waits on memory
   int cur = hdr.x, rbase = cur;
-  int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+  auto rowend = [&](int r) { return r <= a.rows ? __ldg(a.ptr + r) : 0x7fffffff; };
+  int myend = rowend(rbase + 1 + sl);
+  int myend2 = rowend(rbase + SG + 1 + sl);
   int pe = __shfl_sync(sgmask, myend, 0, SG);
   auto finish_and_advance = [&]() {
     if (cur == hdr.x && hdr.z >= 0) {
@@ -315,8 +324,9 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
     for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
     ++cur;
     if (cur - rbase >= SG) {
-      rbase = cur;
-      myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
+      rbase += SG;
+      myend = myend2;
+      myend2 = rowend(rbase + SG + 1 + sl);
     }
     pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
   };
