@@ -237,6 +237,22 @@ def run_cpu_samples(cs, seconds, warm=1):
 
 
 # ------------------------------------------------------------------------------------ ours
+def max_over_ranks(value, dist, device="cuda"):
+    """The largest of every rank's value (a device time: the job takes as long as its slowest
+    replica).  dist is torch.distributed or None (one process)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(work_per_rank, world, seconds):
+    """Aggregate throughput of `world` replicas that each did `work_per_rank` in `seconds`."""
+    return world * work_per_rank / seconds if seconds > 0 else 0.0
+
+
 def _timed(fn, steps, warmup):
     """Device ms per call of fn (CUDA events on the current stream, after warm-up)."""
     import torch
@@ -425,12 +441,9 @@ def run_batch(args):
     torch.cuda.synchronize()
     clocks = sampler.stop(w0, time.time())
     ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     ms_step = ms / args.steps
-    value = world * flops * args.steps / (ms / 1e3) / 1e9
+    value = whole_job_rate(flops * args.steps, world, ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
     # end to end: every member's B in from pinned host memory, every C out, one launch
@@ -450,10 +463,8 @@ def run_batch(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
+    e2e_ms = max_over_ranks(e2e_ms, dist)
     if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
@@ -538,13 +549,10 @@ def run_ours(args):
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     ms_step = ms / args.steps
     flops = 2.0 * nnz * N
-    value = world * flops * args.steps / (ms / 1e3) / 1e9
+    value = whole_job_rate(flops * args.steps, world, ms / 1e3) / 1e9
     esz = B.element_size()
     vsz = 8 if val.dtype == torch.float64 else 4
     alg_bytes = nnz * (vsz + 4) + K * N * esz + M * N * esz
@@ -630,10 +638,7 @@ def run_ours(args):
     t1.record(s_out)
     torch.cuda.synchronize()
     e2e_ms = t0.elapsed_time(t1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist)
     e2e_value = world * flops * args.e2e_steps / (e2e_ms / 1e3) / 1e9
 
     cpu = None
