@@ -257,6 +257,47 @@ SWIFT_COMPAT_SPMM(Swift_GPU_3, 3, "Swift GPU (3.0) SpMM")
 SWIFT_COMPAT_SPMM(Swift_GPU_4, 4, "Swift GPU (4.0) SpMM")
 #undef SWIFT_COMPAT_SPMM
 
+/* ---------------------------------------------------------------- driver helpers
+ * src/auxiliary.h:28-50: the best of the three wrapper times, ignoring failed ones (-1).  All
+ * three failed: -1.  Exactly one valid: the reference matches none of its cases and leaves
+ * time_final as it was; so does this. */
+inline void result_check(float time_Swift_gpu, float time_Swift_gpu1, float time_Swift_gpu2,
+                         float &time_final) {
+  const float t[3] = {time_Swift_gpu, time_Swift_gpu1, time_Swift_gpu2};
+  int failed = 0;
+  float best = 0.f;
+  bool any = false;
+  for (float x : t) {
+    if (x == -1) {
+      ++failed;
+    } else {
+      best = any ? std::fmin(best, x) : x;
+      any = true;
+    }
+  }
+  if (failed == 3) time_final = -1;
+  else if (failed <= 1) time_final = best;
+}
+
+/* src/auxiliary.h:53-64: targetmtx (cols x rows, row-major) = the transpose of originmtx
+ * (rows x cols, row-major); the drivers use it to turn row-major B into the column-major
+ * operand of the GPU wrappers and back. */
+template <class T>
+inline void dense_mtx2dense_mtx_spmm(int rows, int cols, T *originmtx, T *targetmtx) {
+  for (int i = 0; i < cols; ++i)
+    for (int j = 0; j < rows; ++j) targetmtx[(size_t)i * rows + j] = originmtx[(size_t)j * cols + i];
+}
+
+/* src/auxiliary.h:156-165: counts the positions where |resultB - resultA| > 1e-2 into result
+ * (added to its current value, as in the reference). */
+template <class T>
+inline void ResultVerify(T *resultA, T *resultB, int length, int &result) {
+  for (int i = 0; i < length; ++i) {
+    const T d = resultB[i] - resultA[i];  // difference in the value type, as the reference
+    if (std::fabs(d) > 1e-2) ++result;
+  }
+}
+
 /* ---------------------------------------------------------------- src/format.h:48 */
 inline void Tile_destroy(swift_slide_matrix_f64 *matrix) { swift_slide_free_f64(matrix); }
 inline void Tile_destroy(swift_slide_matrix_f32 *matrix) { swift_slide_free_f32(matrix); }

@@ -56,3 +56,35 @@ def test_driver_runs_reference_chain(fp32, shape, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     assert "NO PASS" not in r.stdout
     assert r.stdout.count("GFLOP/s") == 5
+
+
+HELPERS = r'''
+#include <cstdio>
+#include "swift_compat.h"
+int main() {
+  float t = 7.f;
+  result_check(3.f, 2.f, 5.f, t); if (t != 2.f) return 1;
+  result_check(-1.f, 2.f, 5.f, t); if (t != 2.f) return 2;
+  result_check(4.f, -1.f, 3.f, t); if (t != 3.f) return 3;
+  result_check(-1.f, -1.f, -1.f, t); if (t != -1.f) return 4;
+  t = 9.f; result_check(-1.f, -1.f, 5.f, t); if (t != 9.f) return 5;  // one valid: unchanged
+  double a[6] = {1, 2, 3, 4, 5, 6}, b[6];
+  dense_mtx2dense_mtx_spmm(2, 3, a, b);  // 2 x 3 -> 3 x 2
+  const double want[6] = {1, 4, 2, 5, 3, 6};
+  for (int i = 0; i < 6; ++i) if (b[i] != want[i]) return 6;
+  float x[3] = {0.f, 1.f, 2.f}, y[3] = {0.f, 1.005f, 2.5f};
+  int err = 1;
+  ResultVerify(x, y, 3, err); if (err != 2) return 7;
+  return 0;
+}
+'''
+
+
+def test_driver_helpers_match_the_reference_semantics(tmp_path):
+    src = tmp_path / "h.cpp"
+    src.write_text(HELPERS)
+    exe = str(tmp_path / "h")
+    r = subprocess.run([CXX, "-std=c++17", "-Wall", "-Werror", "-I", INCLUDE, str(src), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([exe]).returncode == 0
