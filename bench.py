@@ -13,6 +13,10 @@ Several GPUs run independent replicas (the product has no exchange step).
 --impl reference times the reference's own CPU product (Swift_cpu, compiled from the
 reference sources under oracle/_ref; the oracle's restatement if that build is absent) on
 the host cores: each step is a bounded sample of tiles of the same workload.
+
+--impl reference-gpu (context, one GPU) runs the reference's own GPU SpMM wrappers, compiled
+from its sources for sm_100a under oracle/_ref, on the same workload and times the library's
+product beside them in the same process.
 """
 from __future__ import annotations
 
@@ -787,12 +791,104 @@ def run_reference_batch(args, wl, dev):
     print(json.dumps(out), flush=True)
 
 
+def run_reference_gpu(args):
+    """Context: the reference's own GPU SpMM wrappers (Swift_GPU, Swift_gpu1, Swift_gpu2,
+    Swift_GPU_3, Swift_GPU_4; oracle/_ref/libswiftrefgpu_*.so, compiled from its sources for
+    sm_100a) on this workload, fed the format the reference's own host preprocessing builds.
+    Each wrapper times its kernels with its own CUDA events; `value` is the best variant, as
+    the reference's result_check keeps the best of its variants (src/auxiliary.h:28-50).  The
+    library's autotuned product on the same inputs is timed in the same process beside it."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    import oracle
+    from swift_b200 import Plan
+    wl = WORKLOADS[args.workload]
+    if wl["kind"] not in ("rmat", "rmatband", "poisson") or wl["dtype"] not in ("f32", "f64"):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference's GPU wrappers take FP32 or "
+                          "FP64 B and C of one matrix; this workload is not one"}), flush=True)
+        return
+    if not oracle.ref_gpu_available():
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "oracle/_ref/libswiftrefgpu_*.so not built "
+                          "(needs the reference checkout at build time)"}), flush=True)
+        return
+    torch.cuda.set_device(0)
+    N = wl["N"]
+    M, K, rp, ci, val, B = make_inputs(wl, "cuda")
+    nnz = int(rp[-1])
+    flops = 2.0 * nnz * N
+    vn, Bn = val.cpu().numpy(), B.cpu().numpy()
+    # the library on the same inputs: autotuned product, CUDA events over `steps` launches
+    plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
+    C = torch.empty((M, N), dtype=B.dtype, device="cuda")
+    engine, _ = plan.autotune(B, C)
+    lib_ms = _timed(lambda: plan.spmm(B, C), max(5, min(args.steps, 200)), args.warmup)
+    plan.spmm(B, C)
+    golden = C.cpu().numpy()
+    plan.close()
+    del C
+    torch.cuda.empty_cache()
+    t0 = time.time()
+    with _StdoutToStderr():
+        r, p, cnt, v = oracle.csr2csc(M, K, rp, ci, vn, impl="ref")
+        sr, sv, sn, sB = oracle.col_sort(K, N, cnt, oracle.perm_stable(cnt), p, r, v, B=Bn, impl="ref")
+        del r, v
+        sl = oracle.build(sr, sv, sn, M, K, impl="ref", row_sort=True, N=N)
+    prep_s = time.time() - t0
+    fmt = dict(sl.arrays, tilenum=sl.tilenum, regular_nnz=sl.regular_nnz, reside_col=sl.reside_col,
+               reside_nnz=sl.reside_nnz, segsum=sl.segsum, numblk=sl.numblk)
+    fmt4 = dict(fmt, sortrowidx=sl.arrays["rowsorted_rowidx"])
+    reps = max(1, min(args.steps, 5))
+    variants = {}
+    for var, name in oracle.REF_GPU_VARIANTS.items():
+        f = fmt4 if var == 4 else fmt
+        if not oracle.ref_gpu_accepts(var, f, N, sB.dtype):
+            variants[name] = {"status": "not run: outside the inputs whose launches stay in bounds "
+                                        "(oracle/ref_gpu.cu)"}
+            continue
+        times, st, Cr = [], 0, None
+        with _StdoutToStderr():
+            for i in range(1 + reps):  # the first call warms up
+                st, ms, Cr = oracle.ref_gpu_spmm(var, f, M, K, N, nnz, sB, golden)
+                if st != oracle.REF_GPU_OK:
+                    break
+                if i:
+                    times.append(ms)
+        if st != oracle.REF_GPU_OK:
+            variants[name] = {"status": {1: "reference check failed", 2: "refused",
+                                         3: "CUDA error"}.get(st, str(st))}
+            continue
+        ms = statistics.median(times)
+        diff = float(np.abs(np.asarray(Cr, np.float64) - golden).max() / max(np.abs(golden).max(), 1e-300))
+        variants[name] = {"status": "ok (reference check passed)", "ms": ms, "gflops": flops / (ms / 1e3) / 1e9,
+                          "max_rel_diff_vs_library": diff}
+    ok = [x for x in variants.values() if "ms" in x]
+    best = min(ok, key=lambda x: x["ms"]) if ok else None
+    out = {
+        "metric": "spmm_gflops", "value": best["gflops"] if best else None, "unit": "GFLOP/s",
+        "impl": "reference_gpu", "n_gpus": 1, "steps": reps, "warmup": 1,
+        "ms_per_step": best["ms"] if best else None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": wl["dtype"],
+        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
+                   "cols": K, "nnz": nnz, "N": N, "reference_host_preprocessing_s": prep_s},
+        "timing": "each wrapper's own CUDA events around its kernels; uploads, downloads and its host-side "
+                  "check outside; median of the calls after the first",
+        "variants": variants,
+        "library": {"engine": engine, "ms": lib_ms, "gflops": flops / (lib_ms / 1e3) / 1e9,
+                    "speedup_vs_best_reference_kernel": (best["ms"] / lib_ms) if best else None},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -803,6 +899,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference-gpu":
+        run_reference_gpu(args)
     else:
         run_ours(args)
 

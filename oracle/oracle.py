@@ -10,6 +10,9 @@ Two implementations sit behind the same Python functions:
 * ``impl="ref"``    -- the reference's own host code compiled in place from its checkout
   (``oracle/_ref/libswiftref_{f32,f64}.so``, built by ``oracle/Makefile``), used to pin the
   restatement and as the reference CPU baseline.
+
+``ref_gpu_spmm`` runs the reference's own GPU SpMM wrappers (``oracle/_ref/libswiftrefgpu_*.so``,
+compiled in place for sm_100a) -- a context measurement and a cross-check, never the product.
 """
 from __future__ import annotations
 
@@ -373,3 +376,68 @@ class CpuSwift:
         sec = time.perf_counter() - a
         nnz = (t1 - t0) * 32 + (int(self.s.reside_nnz) if with_reside else 0)
         return sec, nnz
+
+
+# ---------------------------------------------------------------- reference GPU wrappers
+REF_GPU_VARIANTS = {0: "Swift_GPU", 1: "Swift_gpu1", 2: "Swift_gpu2", 3: "Swift_GPU_3", 4: "Swift_GPU_4"}
+REF_GPU_OK, REF_GPU_CHECK_FAILED, REF_GPU_REFUSED, REF_GPU_CUDA_ERROR = 0, 1, 2, 3
+
+
+def ref_gpu_available() -> bool:
+    return all(os.path.exists(os.path.join(HERE, "_ref", f"libswiftrefgpu{s}.so")) for s in ("_f32", "_f64"))
+
+
+def ref_gpu_accepts(variant, arrays, N, dt) -> bool:
+    """The inputs the reference-GPU entry point accepts (oracle/ref_gpu.cu states why)."""
+    T, RN = int(arrays["tilenum"]), int(arrays["reside_nnz"])
+    if N <= 0 or N % 32 or T <= 0 or RN <= 0:
+        return False
+    if variant == 4 and (np.dtype(dt) == np.float64 or T % 8 or "val_position" not in arrays):
+        return False
+    if variant != 1 and int(arrays.get("numblk", 0)) <= 0:
+        return False
+    return True
+
+
+def ref_gpu_spmm(variant, arrays, M, K, N, nnz, B, golden):
+    """One call of the reference's GPU wrapper ``REF_GPU_VARIANTS[variant]`` on the format
+    ``arrays`` (a swift_b200 Plan.export() dict; variant 4 needs the row-sorted export).
+
+    B: sorted dense operand K x N (any order; passed column-major except to Swift_gpu2, which
+    takes it row-major); golden: row-major M x N.  Returns (status, ms, C as M x N), ms being
+    the wrapper's own CUDA-event time of its kernels."""
+    dt = _dt(B.dtype)
+    key = ("refgpu", dt)
+    if key not in _LIBS:
+        _LIBS[key] = C.CDLL(os.path.join(HERE, "_ref", f"libswiftrefgpu{_SFX[dt]}.so"), mode=C.RTLD_LOCAL)
+    lib = _LIBS[key]
+    S = _SLIDE[dt]
+    s = S()
+    keep = []
+
+    def put(name, arr, ct=C.c_int):
+        a = np.ascontiguousarray(arr)
+        if a.size == 0:
+            a = np.zeros(1, a.dtype)
+        keep.append(a)
+        setattr(s, name, a.ctypes.data_as(C.POINTER(ct)))
+
+    for k in ("tilenum", "regular_nnz", "reside_col", "reside_nnz", "segsum", "numblk"):
+        setattr(s, k, int(arrays.get(k, 0)))
+    for k in ("tile_ptr", "tile_len", "tile_colidx", "tile_tall", "sortrowidx", "reside_cscptr",
+              "reside_cscrowidx", "tile_format", "countrow", "segmentoffset", "sortrowindex", "blkstart",
+              "blkstop", "blkptr", "val_position", "val_offset"):
+        if k in arrays:
+            put(k, arrays[k].astype(np.int32))
+    put("sortval", arrays["sortval"].astype(dt), _CT[dt])
+    put("reside_val", arrays["reside_val"].astype(dt), _CT[dt])
+    if "colorblk" in arrays:
+        put("colorblk", arrays["colorblk"].astype(np.uint32), C.c_uint)
+    Bm = np.ascontiguousarray(B, dt) if variant == 2 else np.asfortranarray(B, dt)
+    Cm = np.zeros((M, N), dt, order="C" if variant == 2 else "F")
+    gold = np.ascontiguousarray(golden, dt)
+    ms = C.c_float(0)
+    fn = getattr(lib, "refgpu_spmm" + _SFX[dt])
+    st = fn(int(variant), C.byref(s), M, K, N, int(nnz), _p(Bm, _CT[dt]), _p(Cm, _CT[dt]), _p(gold, _CT[dt]),
+            C.byref(ms))
+    return int(st), float(ms.value), Cm
