@@ -14,6 +14,9 @@ Several GPUs run independent replicas (the product has no exchange step).
 reference sources under oracle/_ref; the oracle's restatement if that build is absent) on
 the host cores: each step is a bounded sample of tiles of the same workload.
 
+--mtx FILE [--n N] [--dtype f32|f64] runs the same product on a MatrixMarket file (the
+reference's input format) instead of a synthetic matrix.
+
 --impl reference-gpu (context, one GPU) runs the reference's own GPU SpMM wrappers, compiled
 from its sources for sm_100a under oracle/_ref, on the same workload and times the library's
 product beside them in the same process.
@@ -62,6 +65,9 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def describe(name, wl, nnz):
+    if wl["kind"] == "mtx":
+        return (f"MatrixMarket file {os.path.basename(wl['path'])} read as the reference's reader reads it "
+                f"({nnz} nnz), the file's values; B {wl['N']} columns U[-1,1] row-major; C = A*B {wl['dtype']}")
     if wl["kind"] == "rmat":
         M = 1 << wl["scale"]
         return (f"R-MAT scale {wl['scale']} ({M}x{M}, {wl['edges']} edge draws, a,b,c,d=.57,.19,.19,.05, "
@@ -75,12 +81,23 @@ def describe(name, wl, nnz):
             f"{nnz} nnz; B {wl['K']}x{wl['N']} U[-1,1]")
 
 
+def data_desc(wl):
+    if wl["kind"] == "mtx":
+        return f"MatrixMarket file {os.path.basename(wl['path'])} (its pattern and values); B synthetic U[-1,1]"
+    return "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)"
+
+
 def make_inputs(wl, device, seed=0):
     """Pattern and values (host numpy CSR) plus B on `device` (torch)."""
     import torch
 
     from swift_b200 import gen
-    if wl["kind"] == "rmat":
+    mtx_val = None
+    if wl["kind"] == "mtx":
+        from swift_b200.mtx import read_mtx
+        mm = read_mtx(wl["path"], np.float64 if wl["dtype"] == "f64" else np.float32)
+        M, K, rp, ci, mtx_val = mm.rows, mm.cols, mm.rowptr, mm.colidx, mm.val
+    elif wl["kind"] == "rmat":
         rp, ci = gen.rmat(wl["scale"], wl["edges"], seed=seed, device=device)
         M = K = 1 << wl["scale"]
     elif wl["kind"] == "rmatband":
@@ -94,6 +111,8 @@ def make_inputs(wl, device, seed=0):
     g.manual_seed(seed + 1)
     vdt = torch.float64 if wl["dtype"] == "f64" else torch.float32
     val = (torch.rand(nnz, generator=g, device=device, dtype=vdt) * 2 - 1)
+    if mtx_val is not None:
+        val = torch.from_numpy(mtx_val).to(device=device, dtype=vdt)
     g.manual_seed(seed + 2)
     if wl["dtype"] == "f64":
         B = torch.rand((K, wl["N"]), generator=g, device=device, dtype=torch.float64) * 2 - 1
@@ -669,7 +688,7 @@ def run_ours(args):
         "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
-        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "data": data_desc(wl),
         "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz),
                    "rows": M, "cols": K, "nnz": nnz, "N": N, "engine": engine,
                    "row_engine_params": rw_params,
@@ -745,7 +764,7 @@ def run_reference(args):
         "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot_s * 1e3 / max(1, args.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"], "impl": "reference",
-        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "data": data_desc(wl),
         "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
                    "cols": K, "nnz": nnz, "N": N, "parallelism": "host CPU, rank 0 only"},
         "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": 1,
@@ -806,7 +825,7 @@ def run_reference_gpu(args):
     import oracle
     from swift_b200 import Plan
     wl = WORKLOADS[args.workload]
-    if wl["kind"] not in ("rmat", "rmatband", "poisson") or wl["dtype"] not in ("f32", "f64"):
+    if wl["kind"] not in ("rmat", "rmatband", "poisson", "mtx") or wl["dtype"] not in ("f32", "f64"):
         print(json.dumps({"impl": "reference_gpu", "unavailable": "the reference's GPU wrappers take FP32 or "
                           "FP64 B and C of one matrix; this workload is not one"}), flush=True)
         return
@@ -871,7 +890,7 @@ def run_reference_gpu(args):
         "impl": "reference_gpu", "n_gpus": 1, "steps": reps, "warmup": 1,
         "ms_per_step": best["ms"] if best else None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": wl["dtype"],
-        "data": "synthetic (seeded generator; the reference's SuiteSparse inputs are not available offline)",
+        "data": data_desc(wl),
         "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
                    "cols": K, "nnz": nnz, "N": N, "reference_host_preprocessing_s": prep_s},
         "timing": "each wrapper's own CUDA events around its kernels; uploads, downloads and its host-side "
@@ -894,7 +913,15 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mtx", help="MatrixMarket coordinate file: run the product on this matrix instead "
+                                  "of a synthetic workload")
+    ap.add_argument("--n", type=int, default=128, help="dense columns with --mtx")
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f32", help="value type with --mtx")
     args = ap.parse_args()
+    if args.mtx:
+        name = f"mtx:{os.path.splitext(os.path.basename(args.mtx))[0]}_n{args.n}_{args.dtype}"
+        WORKLOADS[name] = dict(kind="mtx", path=args.mtx, N=args.n, dtype=args.dtype)
+        args.workload = name
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":

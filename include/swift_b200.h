@@ -65,7 +65,9 @@ typedef enum swift_status {
   SWIFT_ERR_OVERFLOW = 7,    /* a size exceeds the int32 index range of the format        */
   SWIFT_ERR_TIMEOUT = 8,     /* a bounded device-side wait ran out                        */
   SWIFT_ERR_NO_DEVICE = 9,   /* no CUDA device, or not an sm_100 device                   */
-  SWIFT_ERR_VERIFY = 10      /* compat entry points: result differs from the golden C     */
+  SWIFT_ERR_VERIFY = 10,     /* compat entry points: result differs from the golden C     */
+  SWIFT_ERR_IO = 11,         /* a file cannot be opened or read                           */
+  SWIFT_ERR_FORMAT = 12      /* a MatrixMarket file is malformed                          */
 } swift_status;
 
 typedef enum swift_dtype { SWIFT_F32 = 0, SWIFT_F64 = 1, SWIFT_BF16 = 2, SWIFT_F16 = 3 } swift_dtype;
@@ -319,6 +321,23 @@ swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream);
  * (operands must be set; each C_i is overwritten with its product). */
 swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, double *best_ms,
                                   int *best_task_size);
+
+/* ------------------------------------------------------------------ MatrixMarket input */
+/* Reads a MatrixMarket coordinate file into host CSR as the reference's reader does
+ * (mmio_allinone, src/auxiliary.h:167-332): 0-based indices, entries in file order inside
+ * each row (duplicates kept), off-diagonal entries of symmetric and hermitian files mirrored
+ * with the same value, skew-symmetric files read as stored, pattern entries 1.0, complex
+ * entries their real part.  val_type is SWIFT_F32 or SWIFT_F64.  *rowptr (m + 1), *colidx and
+ * *val (nnz) are malloc'd; release each with swift_host_free.  Errors: SWIFT_ERR_IO (cannot
+ * open or read), SWIFT_ERR_FORMAT (banner, size line or an entry malformed, an index outside
+ * the matrix), SWIFT_ERR_UNSUPPORTED ("array" files), SWIFT_ERR_OVERFLOW.  reference_code
+ * (may be NULL) receives what the reference's reader returns for the file: 0, -1 (cannot
+ * open), -2 (banner), -4 (size line), or -5 where the reference would go on with undefined
+ * values. */
+swift_status swift_mtx_read(const char *path, swift_dtype val_type, int *m, int *n, int *nnz,
+                            int *is_symmetric, int **rowptr, int **colidx, void **val,
+                            int *reference_code);
+void swift_host_free(void *p);
 
 /* ------------------------------------------------------------------ reference calling convention */
 /* The reference's preprocessing and kernels with its host-buffer convention: inputs and

@@ -298,6 +298,38 @@ inline void ResultVerify(T *resultA, T *resultB, int length, int &result) {
   }
 }
 
+/* ---------------------------------------------------------------- src/auxiliary.h:167-332
+ * MatrixMarket coordinate file -> CSR in malloc'd arrays (the caller frees them with free(), as
+ * the reference's callers do), through swift_mtx_read.  Returns the reference's codes: 0,
+ * -1 (cannot open), -2 (banner; prints the reference's message), -4 (size line); and -5 where
+ * the reference would go on with undefined values (an index outside the matrix, a missing
+ * or malformed entry, an "array" file). */
+namespace swift_compat_detail {
+template <class T>
+inline int mmio(int *m, int *n, int *nnz, int *isSymmetric, int **csrrowptr, int **csrcolidx,
+                T **csrval, const char *filename, swift_dtype dt) {
+  int code = 0;
+  void *v = nullptr;
+  const swift_status s = swift_mtx_read(filename, dt, m, n, nnz, isSymmetric, csrrowptr, csrcolidx, &v, &code);
+  if (s != SWIFT_OK) {
+    if (code == -2) std::printf("Could not process Matrix Market banner.\n");
+    else report(s, "mmio_allinone");
+    return code ? code : -5;
+  }
+  *csrval = static_cast<T *>(v);
+  return 0;
+}
+}  // namespace swift_compat_detail
+
+inline int mmio_allinone(int *m, int *n, int *nnz, int *isSymmetric, int **csrrowptr, int **csrcolidx,
+                         double **csrval, char *filename) {
+  return swift_compat_detail::mmio(m, n, nnz, isSymmetric, csrrowptr, csrcolidx, csrval, filename, SWIFT_F64);
+}
+inline int mmio_allinone(int *m, int *n, int *nnz, int *isSymmetric, int **csrrowptr, int **csrcolidx,
+                         float **csrval, char *filename) {
+  return swift_compat_detail::mmio(m, n, nnz, isSymmetric, csrrowptr, csrcolidx, csrval, filename, SWIFT_F32);
+}
+
 /* ---------------------------------------------------------------- src/format.h:48 */
 inline void Tile_destroy(swift_slide_matrix_f64 *matrix) { swift_slide_free_f64(matrix); }
 inline void Tile_destroy(swift_slide_matrix_f32 *matrix) { swift_slide_free_f32(matrix); }

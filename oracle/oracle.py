@@ -441,3 +441,25 @@ def ref_gpu_spmm(variant, arrays, M, K, N, nnz, B, golden):
     st = fn(int(variant), C.byref(s), M, K, N, int(nnz), _p(Bm, _CT[dt]), _p(Cm, _CT[dt]), _p(gold, _CT[dt]),
             C.byref(ms))
     return int(st), float(ms.value), Cm
+
+
+# ---------------------------------------------------------------- reference MatrixMarket reader
+def ref_mmio(path):
+    """The reference's own mmio_allinone (src/auxiliary.h:167-332, FP64 build) on a file.
+    Returns (return code, rows, cols, is_symmetric, rowptr, colidx, val); the arrays are None
+    unless the code is 0.  Only for well-formed files, a missing file or a bad banner (its
+    size-line loop does not end on other malformed input)."""
+    lib = _lib("ref", np.float64)
+    m, n, nnz, sym = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+    rp, ci, vv = _I(), _I(), C.POINTER(C.c_double)()
+    fn = lib.ref_mmio_allinone_f64
+    fn.restype = C.c_int
+    rc = fn(os.fsencode(path), C.byref(m), C.byref(n), C.byref(nnz), C.byref(sym), C.byref(rp), C.byref(ci),
+            C.byref(vv))
+    if rc != 0:
+        return rc, 0, 0, 0, None, None, None
+    out = (rc, m.value, n.value, sym.value, _arr(rp, m.value + 1, np.int32), _arr(ci, nnz.value, np.int32),
+           _arr(vv, nnz.value, np.float64))
+    for p in (rp, ci, vv):
+        lib.ref_host_free(C.cast(p, C.c_void_p))
+    return out

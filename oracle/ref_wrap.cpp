@@ -239,4 +239,16 @@ double REFN(ref_swift_cpu_tiles)(const or_slide_t *m, int t0, int t1, int with_r
   return (b.tv_sec - a.tv_sec) * 1000.0 + (b.tv_usec - a.tv_usec) / 1000.0;
 }
 
+#if defined(REF_FP64)
+// The reference's MatrixMarket reader (src/auxiliary.h:167-332) as it stands.  FP64 build only:
+// the FP32 copy passes a float to "%lg" (test/k-32/FP32/auxiliary.h:65), which writes a double
+// into it.  Callers feed it well-formed files, a missing file or a bad banner only: on other
+// malformed input its size-line loop does not end (src/mmio.h:162-167).
+int ref_mmio_allinone_f64(const char *path, int *m, int *n, int *nnz, int *is_symmetric, int **rowptr,
+                          int **colidx, double **val) {
+  return mmio_allinone(m, n, nnz, is_symmetric, rowptr, colidx, val, const_cast<char *>(path));
+}
+void ref_host_free(void *p) { free(p); }
+#endif
+
 }  // extern "C"

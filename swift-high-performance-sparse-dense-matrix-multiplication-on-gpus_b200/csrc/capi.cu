@@ -95,6 +95,8 @@ const char *swift_status_string(swift_status s) {
     case SWIFT_ERR_TIMEOUT: return "bounded device wait timed out";
     case SWIFT_ERR_NO_DEVICE: return "no sm_100 CUDA device";
     case SWIFT_ERR_VERIFY: return "result differs from the golden product";
+    case SWIFT_ERR_IO: return "file cannot be opened or read";
+    case SWIFT_ERR_FORMAT: return "malformed MatrixMarket file";
   }
   return "unknown status";
 }

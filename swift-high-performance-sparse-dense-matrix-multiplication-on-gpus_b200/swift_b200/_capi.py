@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libswiftb200.so")
 
 # enums (include/swift_b200.h)
 OK, ERR_INVALID_ARG, ERR_BAD_CSR, ERR_BAD_PERM, ERR_UNSUPPORTED, ERR_CUDA, ERR_ALLOC, \
-    ERR_OVERFLOW, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_VERIFY = range(11)
+    ERR_OVERFLOW, ERR_TIMEOUT, ERR_NO_DEVICE, ERR_VERIFY, ERR_IO, ERR_FORMAT = range(13)
 F32, F64, BF16, F16 = 0, 1, 2, 3
 ROW_MAJOR, COL_MAJOR = 0, 1
 HOST, DEVICE = 0, 1
@@ -146,6 +146,9 @@ _SIGS = [
     ("swift_batch_run", C.c_int, [_P, _P]),
     ("swift_batch_run_graph", C.c_int, [_P, _P]),
     ("swift_batch_autotune", C.c_int, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("swift_mtx_read", C.c_int, [C.c_char_p, C.c_int] + [C.POINTER(C.c_int)] * 4
+     + [C.POINTER(C.POINTER(C.c_int))] * 2 + [C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
+    ("swift_host_free", None, [_P]),
 ]
 # reference-convention functions (host buffers), one per value type
 _FP = C.POINTER(C.c_float)

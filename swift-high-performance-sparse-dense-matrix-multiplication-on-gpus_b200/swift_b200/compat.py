@@ -14,6 +14,9 @@ stage on the GPU.  Names, argument meanings and the order of calls follow the re
     blockratio = row_idx_sort(mat, rowA, colA, width)
     C, ms = Swift_GPU_4(mat, rowA, colA, width, nnz, sdense_colmajor)
 
+The driver's input comes from ``mmio_allinone(filename)`` (src/auxiliary.h:167-332), which
+returns the reference's code with the CSR: ``rc, m, n, nnz, isSymmetric, rowptr, colidx, val``.
+
 SpMM wrappers take the column-sorted dense operand and return C in the wrapper's own layout:
 column-major (numpy Fortran order, M x N) for Swift_GPU / Swift_gpu1 / Swift_GPU_3 / Swift_GPU_4
 and row-major for Swift_gpu2, as the reference wrappers do (src/main.cu:338-340).
@@ -215,3 +218,16 @@ def Swift_GPU_3(m, rowA, colA, width, nnz, sort_dense):
 def Swift_GPU_4(m, rowA, colA, width, nnz, sort_dense):
     """src/Swift_4.h:305 (column-major; after row_idx_sort, slot rows via val_position) -> (C, ms)."""
     return _spmm(4, m, rowA, colA, width, nnz, sort_dense)
+
+
+def mmio_allinone(filename, dtype=np.float64):
+    """src/auxiliary.h:167-332 -> (rc, m, n, nnz, isSymmetric, csrrowptr, csrcolidx, csrval).
+
+    rc is the reference's return code (0, -1 cannot open, -2 banner, -4 size line) or -5 where
+    the reference would go on with undefined values; the arrays are None unless rc == 0."""
+    from .mtx import read_mtx, reference_code
+    try:
+        mm = read_mtx(filename, dtype)
+    except capi.SwiftError:
+        return reference_code(filename) or -5, 0, 0, 0, 0, None, None, None
+    return 0, mm.rows, mm.cols, mm.nnz, int(mm.symmetric), mm.rowptr, mm.colidx, mm.val

@@ -58,6 +58,14 @@ class Plan:
 
     # ------------------------------------------------------------------ construction
     @classmethod
+    def from_mtx(cls, path, dtype=np.float32, **kw):
+        """A plan over the matrix of a MatrixMarket coordinate file (swift_b200.mtx.read_mtx,
+        the reference reader's CSR); keyword arguments as for from_csr."""
+        from .mtx import read_mtx
+        m = read_mtx(path, dtype)
+        return cls.from_csr(m.rowptr, m.colidx, m.val, m.shape, **kw)
+
+    @classmethod
     def from_csr(cls, rowptr, colidx, val, shape, col_perm=None, long_row_split=0,
                  build_transpose=False, stream=None):
         torch = _torch()

@@ -88,3 +88,39 @@ def test_driver_helpers_match_the_reference_semantics(tmp_path):
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert subprocess.run([exe]).returncode == 0
+
+
+MMIO = r"""
+#include <cstdio>
+#include <cstdlib>
+#include "swift_compat.h"
+int main(int argc, char **argv) {
+  int m, n, nnz, sym, *rp, *ci;
+  double *v;
+  if (mmio_allinone(&m, &n, &nnz, &sym, &rp, &ci, &v, argv[1]) != 0) return 1;
+  // 3 x 3 symmetric: (1,1)=2, (3,1)=-1 -> row 0: [0]=2, [2]=-1; row 2: [0]=-1
+  if (m != 3 || n != 3 || nnz != 3 || sym != 1) return 2;
+  if (rp[0] != 0 || rp[1] != 2 || rp[2] != 2 || rp[3] != 3) return 3;
+  if (ci[0] != 0 || ci[1] != 2 || ci[2] != 0 || v[0] != 2.0 || v[1] != -1.0 || v[2] != -1.0) return 4;
+  free(rp); free(ci); free(v);
+  float *f;
+  if (mmio_allinone(&m, &n, &nnz, &sym, &rp, &ci, &f, argv[1]) != 0 || f[1] != -1.0f) return 5;
+  free(rp); free(ci); free(f);
+  if (mmio_allinone(&m, &n, &nnz, &sym, &rp, &ci, &v, argv[2]) != -1) return 6;   // missing file
+  return 0;
+}
+"""
+
+
+def test_mmio_allinone_shim(tmp_path):
+    if not os.path.exists(os.path.join(LIBDIR, "libswiftb200.so")):
+        pytest.skip("library not built")
+    mtx = tmp_path / "a.mtx"
+    mtx.write_text("%%MatrixMarket matrix coordinate real symmetric\n3 3 2\n1 1 2.0\n3 1 -1.0\n")
+    src = tmp_path / "m.cpp"
+    src.write_text(MMIO)
+    exe = str(tmp_path / "m")
+    r = subprocess.run([CXX, "-std=c++17", "-Wall", "-Werror", "-I", INCLUDE, str(src), "-o", exe, "-L", LIBDIR,
+                        "-lswiftb200", "-Wl,-rpath," + LIBDIR], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([exe, str(mtx), str(tmp_path / "absent.mtx")]).returncode == 0
