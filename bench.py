@@ -56,6 +56,11 @@ WORKLOADS = {
     "fwdbwd_rmat18sym_n64": dict(kind="fwdbwd", scale=18, edges=(32 << 18) // 2, N=64, dtype="f32"),
     # the batching workload: 512 independent products in one persistent launch
     "batch512_f32": dict(kind="batch", count=512, N=None, dtype="f32"),
+    # standalone SDDMM (out[e] = U[row e] . V[col e]) at the dense widths of the reference's SDDMM
+    # comparison scripts (32 and 128), on the scale matrix
+    "sddmm_rmat20_n32_f32": dict(kind="sddmm", scale=20, edges=16 << 20, N=32, dtype="f32"),
+    "sddmm_rmat20_n128_f32": dict(kind="sddmm", scale=20, edges=16 << 20, N=128, dtype="f32"),
+    "sddmm_rmat19_n128_f32": dict(kind="sddmm", scale=19, edges=8 << 20, N=128, dtype="f32"),
     # the 4096 x 4096 parity workload (rows ~Poisson(16))
     "poisson4096_n32_f32": dict(kind="poisson", M=4096, K=4096, lam=16.0, N=32, dtype="f32"),
 }
@@ -68,8 +73,11 @@ def describe(name, wl, nnz):
     if wl["kind"] == "mtx":
         return (f"MatrixMarket file {os.path.basename(wl['path'])} read as the reference's reader reads it "
                 f"({nnz} nnz), the file's values; B {wl['N']} columns U[-1,1] row-major; C = A*B {wl['dtype']}")
-    if wl["kind"] == "rmat":
+    if wl["kind"] in ("rmat", "sddmm"):
         M = 1 << wl["scale"]
+        if wl["kind"] == "sddmm":
+            return (f"SDDMM on R-MAT scale {wl['scale']} ({M}x{M}, {wl['edges']} edge draws, duplicates merged -> "
+                    f"{nnz} nnz): out[e] = U[row e] . V[col e], U and V {M}x{wl['N']} U[-1,1] {wl['dtype']}")
         return (f"R-MAT scale {wl['scale']} ({M}x{M}, {wl['edges']} edge draws, a,b,c,d=.57,.19,.19,.05, "
                 f"duplicates merged -> {nnz} nnz), values U[-1,1]; B {M}x{wl['N']} U[-1,1] row-major; "
                 f"C = A*B {wl['dtype']}")
@@ -97,7 +105,7 @@ def make_inputs(wl, device, seed=0):
         from swift_b200.mtx import read_mtx
         mm = read_mtx(wl["path"], np.float64 if wl["dtype"] == "f64" else np.float32)
         M, K, rp, ci, mtx_val = mm.rows, mm.cols, mm.rowptr, mm.colidx, mm.val
-    elif wl["kind"] == "rmat":
+    elif wl["kind"] in ("rmat", "sddmm"):
         rp, ci = gen.rmat(wl["scale"], wl["edges"], seed=seed, device=device)
         M = K = 1 << wl["scale"]
     elif wl["kind"] == "rmatband":
@@ -345,6 +353,62 @@ def run_precision(args):
     _single_gpu_line(args, out)
 
 
+def run_sddmm(args):
+    """Standalone SDDMM: out[e] = U[row e] . V[col e] for every nonzero e (the backward kernel
+    for dA on its own).  value = 2 nnz N / time; bytes = nnz (index 4 + output s) + U once +
+    V once; the vendor's CSR SDDMM (torch.sparse.sampled_addmm) is timed beside it."""
+    import torch
+
+    from swift_b200 import Plan
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    wl = WORKLOADS[args.workload]
+    M, K, rp, ci, val, _ = make_inputs(wl, "cuda")
+    N = wl["N"]
+    nnz = int(rp[-1])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    U = torch.rand((M, N), generator=g, device="cuda") * 2 - 1
+    V = torch.rand((K, N), generator=g, device="cuda") * 2 - 1
+    plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
+    out = torch.empty(nnz, device="cuda")
+    ms = _timed(lambda: plan.sddmm(U, V, out), args.steps, args.warmup)
+    flops = 2.0 * nnz * N
+    alg_bytes = nnz * (4 + 4) + M * N * 4 + K * N * 4
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    prof = profile_summary(args.workload)
+    traffic = float(prof["dram_bytes_per_launch"].split()[0]) if prof else None
+    library = None
+    try:
+        A_t = torch.sparse_csr_tensor(torch.from_numpy(rp).cuda().long(), torch.from_numpy(ci).cuda().long(),
+                                      torch.zeros(nnz, device="cuda"), size=(M, K))
+        Vt = V.t()
+        lib_ms = _timed(lambda: torch.sparse.sampled_addmm(A_t, U, Vt, beta=0.0, alpha=1.0), 5, 2)
+        ref = torch.sparse.sampled_addmm(A_t, U, Vt, beta=0.0, alpha=1.0).values()
+        diff = float((ref - out).abs().max() / ref.abs().max())
+        library = {"what": "torch.sparse.sampled_addmm on a CSR tensor (cuSPARSE SDDMM)", "ms_per_step": lib_ms,
+                   "gflops": flops / (lib_ms / 1e3) / 1e9, "max_rel_diff": diff}
+        del A_t
+    except Exception as ex:  # context row only
+        library = {"what": "torch.sparse.sampled_addmm on a CSR tensor", "error": str(ex)[:200]}
+    res = {
+        "metric": "sddmm_gflops", "value": flops / (ms / 1e3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": data_desc(wl),
+        "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
+                   "cols": K, "nnz": nnz, "N": N,
+                   "l2": "inputs larger than L2 (U and V exceed 126 MB); no flush between steps"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "traffic_source": prof.get("file"), "kernel": prof.get("kernel", "merge_bwd_kernel"),
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes},
+        "gpu_launches": args.steps,
+        "library_context": library,
+    }
+    _single_gpu_line(args, res)
+    plan.close()
+
+
 def run_fwdbwd(args):
     """The differentiation workload: Y = A X, dX = A^T dY, dA = SDDMM(dY, X) on a symmetric-
     normalised R-MAT graph; fused (one pass over A for Y and dA, then A^T) against the same
@@ -529,6 +593,8 @@ def run_ours(args):
         return run_precision(args)
     if kind == "fwdbwd":
         return run_fwdbwd(args)
+    if kind == "sddmm":
+        return run_sddmm(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -733,6 +799,10 @@ def run_reference(args):
         dev = "cpu"
     if wl["kind"] == "batch":
         return run_reference_batch(args, wl, dev)
+    if wl["kind"] in ("sddmm", "fwdbwd", "precision"):
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference has no CPU path for the "
+                          f"{wl['kind']} workload (SpMM only)"}), flush=True)
+        return
     M, K, rp, ci, val, B = make_inputs(wl, dev)
     import torch
     Bn = B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy()

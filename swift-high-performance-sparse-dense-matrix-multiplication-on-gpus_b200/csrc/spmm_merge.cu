@@ -508,23 +508,28 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
   const int p = (int)(d0 - hdr.x);
   const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
   const bool inb = lsl * VB < a.N;
-  T acc[VB], urow[VB];
+  // dY rows are consumed in row order.  For SDDMM alone (registers to spare) the next row's
+  // vector is fetched when the walk enters a row, so its latency overlaps the current row's
+  // gathers; the fused passes load it on entry.
+  constexpr bool PREU = DODA && !DOY && !DODX;
+  T acc[VB], urow[VB], unext[PREU ? VB : 1];
 #pragma unroll
   for (int e = 0; e < VB; ++e) acc[e] = urow[e] = T(0);
   const T *dYp = static_cast<const T *>(ba.dY);
-  auto load_u = [&](int row) {
+  auto fetch_u = [&](int row, auto &dst) {
     if (DODA) {
-      if (role == 0 && inb && row < a.rows) vload<T, T, VB>(dYp + (int64_t)row * ba.lddy + lsl * VB, urow);
+      if (role == 0 && inb && row < a.rows) vload<T, T, VB>(dYp + (int64_t)row * ba.lddy + lsl * VB, dst);
       else {
 #pragma unroll
-        for (int e = 0; e < VB; ++e) urow[e] = T(0);
+        for (int e = 0; e < VB; ++e) dst[e] = T(0);
       }
     }
   };
   int cur = hdr.x, rbase = cur;
   int myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
   int pe = __shfl_sync(sgmask, myend, 0, SG);
-  load_u(cur);
+  fetch_u(cur, urow);
+  if constexpr (PREU) fetch_u(cur + 1, unext);
   auto finish_and_advance = [&]() {
     if (DOY || DODX) {
       if (cur == hdr.x && hdr.z >= 0) {
@@ -546,7 +551,13 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
       myend = rbase + 1 + sl <= a.rows ? __ldg(a.ptr + rbase + 1 + sl) : 0x7fffffff;
     }
     pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
-    load_u(cur);
+    if constexpr (PREU) {
+#pragma unroll
+      for (int e = 0; e < VB; ++e) urow[e] = unext[e];
+      fetch_u(cur + 1, unext);
+    } else {
+      fetch_u(cur, urow);
+    }
   };
   const char *Gl = role ? reinterpret_cast<const char *>(dYp + lsl * VB)
                         : reinterpret_cast<const char *>(static_cast<const T *>(a.B) + lsl * VB);
@@ -555,6 +566,12 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
   constexpr unsigned LOW = SG == 32 ? 0xffffffffu : ((1u << SG) - 1u);
   const T *val = static_cast<const T *>(a.val);
   T *dA = static_cast<T *>(ba.dA);
+  // SDDMM alone: a slot past the chunk's end holds column 0, so its gather stays in bounds and
+  // its dot product is never stored -- the loads need no slot predicate, and lanes past N keep
+  // the zeros set here (their loads are predicated off).
+  BVec<T, T, VB> x[UNR];
+#pragma unroll
+  for (int u = 0; u < UNR; ++u) x[u].zero();
   for (int q0 = p; q0 < pn; q0 += 32) {
     const int m = min(32, pn - q0);
     unsigned rs = 0;
@@ -576,14 +593,17 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
     }
     __syncwarp(sgmask);
     for (int k = 0; k < m; k += UNR) {
-      BVec<T, T, VB> x[UNR];
       T part[UNR];
 #pragma unroll
       for (int u = 0; u < UNR; ++u) {
-        const bool ok = k + u < m;
-        const uint32_t c = ok ? (uint32_t)stage[k + u].x : 0u;
-        if (inb && ok) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)c * g_ld));
-        else x[u].zero();
+        if constexpr (PREU) {
+          if (inb) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)(uint32_t)stage[k + u].x * g_ld));
+        } else {
+          const bool ok = k + u < m;
+          const uint32_t c = ok ? (uint32_t)stage[k + u].x : 0u;
+          if (inb && ok) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)c * g_ld));
+          else x[u].zero();
+        }
         part[u] = T(0);
       }
       const bool starts = (rs >> k) & 0xFu;
