@@ -283,9 +283,11 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
  * B-row vector loads each lane issues before consuming them (4 = default, with registers
  * capped for 64 resident warps per SM; 8; or 16); vector_bytes = bytes per lane access (0 =
  * widest the operands allow, 32, 16 or 4); kernel = 0 (choose), 1 (lean walk), 2 (walk over
- * row-start-flagged indices staged in shared memory), 3 (general walk, any width).  The
- * override applies to every later swift_spmm with the ROWWISE (or AUTO) engine on this
- * plan. */
+ * row-start-flagged indices staged in shared memory), 3 (general walk, any width), 4 (staged
+ * walk: FP32 operands with N = 32, 64 or 128 and 16-byte vectors; each lane keeps its slices
+ * of the next 7 or 15 gathered B rows -- loads_in_flight 8 or 16 -- in flight through cp.async
+ * into shared memory; other shapes take the walk the other parameters select).  The override applies to
+ * every later swift_spmm with the ROWWISE (or AUTO) engine on this plan. */
 swift_status swift_plan_set_rowwise_params(swift_plan *plan, int task_size, int loads_in_flight,
                                            int vector_bytes, int kernel);
 /* The parameters AUTO / ROWWISE would use for (N, dtype) on this plan. */

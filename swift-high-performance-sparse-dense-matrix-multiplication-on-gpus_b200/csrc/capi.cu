@@ -463,7 +463,7 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
 
 swift_status swift_plan_set_rowwise_params(swift_plan *plan, int task_size, int loads_in_flight,
                                            int vector_bytes, int kernel) {
-  if (!plan || task_size < 0 || kernel < 0 || kernel > 3) return SWIFT_ERR_INVALID_ARG;
+  if (!plan || task_size < 0 || kernel < 0 || kernel > 4) return SWIFT_ERR_INVALID_ARG;
   if (vector_bytes != 0 && vector_bytes != 4 && vector_bytes != 16 && vector_bytes != 32)
     return SWIFT_ERR_INVALID_ARG;
   Plan &p = plan->p;

@@ -138,7 +138,7 @@ struct MergeOpts {
   int U = 512;      // merged positions per task
   int unroll = 4;   // B-row loads in flight per lane and batch (4, 8 or 16)
   int vbytes = 0;   // vector bytes per lane: 0 = widest the operands allow, 32, 16 or 4
-  int kernel = 0;   // 0 choose, 1 lean walk, 2 flagged-index walk, 3 general walk
+  int kernel = 0;   // 0 choose, 1 lean walk, 2 flagged-index walk, 3 general walk, 4 staged walk
 };
 
 struct Plan {

@@ -409,6 +409,188 @@ __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a
   flag_walk<T, TA, ACC, VB, SG, FULL>(a, t, sl, sgmask, stage_all[w], vstage_all[sizeof(TA) == 8 ? w : 0]);
 }
 
+// ---------------------------------------------------------------- staged walk
+// cp.async (16 bytes per lane, completion tracked per thread in commit order).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+
+// Shared memory of the staged walk per 256-thread block: every lane's ring of D 16-byte
+// slots, then per sub-warp a ring of NCH chunks of 32 (index, value) pairs.
+constexpr int staged_nch(int D) { return D / 4 - 1 <= 4 ? 2 : 4; }
+constexpr int staged_smem(int SG, int D) { return 8 * 32 * D * 16 + 8 * (32 / SG) * staged_nch(D) * 32 * 8; }
+constexpr int staged_minb(int SG, int D) {
+  const int b = (227 * 1024) / (staged_smem(SG, D) + 1024);
+  return b < 1 ? 1 : (b > 6 ? 6 : b);
+}
+
+// Staged walk (FP32 values, B and C; N == SG * 4, so every lane holds one 16-byte slice of a
+// row).  Nonzeros go in groups of four (aligned to multiples of 4 in the nonzero order); each
+// lane keeps its slices of the next D / 4 - 1 groups' B rows in flight in a lane-private ring
+// of D slots of shared memory, filled by cp.async -- so the bytes in flight per SM are bounded
+// by shared memory rather than by registers, and one wait, one commit and two 16-byte reads of
+// (indices, values) serve four nonzeros.  Chunks of 32 (index, value) pairs ride the same copy
+// groups into a ring one or two chunks ahead.  Copies complete in commit order: waiting until
+// at most D / 4 - 2 groups are pending makes the current group's slices visible to the lane,
+// and a __syncwarp after the wait that covers a staging copy makes the staged chunk visible to
+// every lane.  The partial groups at the ends of a task take plain loads.  Row bookkeeping,
+// split rows and results are those of the flagged walk.
+template <int SG, int D, int MINB>
+__global__ void __launch_bounds__(256, MINB) merge_staged_kernel(const MergeArgs a) {
+  constexpr int G = 32 / SG;
+  constexpr int LAG = D / 4 - 1;  // groups in flight per lane
+  constexpr int NCH = staged_nch(D);
+  constexpr int SMASK = NCH * 32 - 1;
+  static_assert((D & (D - 1)) == 0 && LAG >= 1 && LAG <= 8, "ring depth");
+  extern __shared__ float4 staged_dyn[];
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
+  if (t >= a.ntasks) return;
+  const int w = (threadIdx.x >> 5) * G + sg;
+  float4 *ring = staged_dyn + (threadIdx.x >> 5) * 32 * D;  // [D][32 lanes] per warp
+  int *sidx = reinterpret_cast<int *>(staged_dyn + 8 * 32 * D) + w * (NCH * 64);
+  float *sval = reinterpret_cast<float *>(sidx + NCH * 32);
+  const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
+  const int64_t d0 = (int64_t)t * a.U;
+  const int p = (int)(d0 - hdr.x);
+  const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
+  const int nnz = (int)(a.total - a.rows);
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  int cur = hdr.x, rbase = cur;
+  auto rowend = [&](int r) { return r <= a.rows ? __ldg(a.ptr + r) : 0x7fffffff; };
+  int myend = rowend(rbase + 1 + sl);
+  int myend2 = rowend(rbase + SG + 1 + sl);
+  int pe = __shfl_sync(sgmask, myend, 0, SG);
+  auto finish_and_advance = [&]() {
+    if (cur == hdr.x && hdr.z >= 0) {
+      float *dst = static_cast<float *>(a.scratch) + (int64_t)(2 * t) * a.N + sl * 4;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) __stcg(dst + e, acc[e]);
+    } else {
+      const int orow = a.out_row ? __ldg(a.out_row + cur) : cur;
+      vstore<float, float, 4>(static_cast<float *>(a.C) + (int64_t)orow * a.ldc + sl * 4, acc);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[e] = 0.f;
+    ++cur;
+    if (cur - rbase >= SG) {
+      rbase += SG;
+      myend = myend2;
+      myend2 = rowend(rbase + SG + 1 + sl);
+    }
+    pe = __shfl_sync(sgmask, myend, cur - rbase, SG);
+  };
+  auto accumulate = [&](float wv, const float4 &b) {
+    const float bv[4] = {b.x, b.y, b.z, b.w};
+    fma_vec<float, 4>(acc, wv, bv);
+  };
+  const char *Bl = reinterpret_cast<const char *>(static_cast<const float *>(a.B) + sl * 4);
+  const uint32_t ldb_bytes = (uint32_t)(a.ldb * (int64_t)sizeof(float));  // < 2^32 (checked at launch)
+  const int *vbits = static_cast<const int *>(a.val);
+  // one nonzero without the pipeline (the partial groups at a task's ends)
+  auto single = [&](int x) {
+    const int c = __ldg(a.idx + x);
+    const float wv = __int_as_float(__ldg(vbits + x));
+    const float4 b = __ldg(reinterpret_cast<const float4 *>(Bl + (uint64_t)(uint32_t)(c & 0x7fffffff) * ldb_bytes));
+    if (c < 0) {
+      while (x == pe) finish_and_advance();
+    }
+    accumulate(wv, b);
+  };
+  const int g0 = (p + 3) >> 2, g1 = pn >> 2;  // full groups [g0, g1)
+  if (g0 >= g1) {
+    for (int x = p; x < pn; ++x) single(x);
+  } else {
+    for (int x = p; x < 4 * g0; ++x) single(x);
+    // chunk k = nonzeros [32k, 32k + 32): 8 pieces of 4 indices, 8 pieces of 4 values
+    auto stage = [&](int k) {
+      for (int pc = sl; pc < 16; pc += SG) {
+        const int part = pc & 7, e0 = 32 * k + part * 4;
+        int *dst = (pc < 8 ? sidx : reinterpret_cast<int *>(sval)) + ((32 * k) & SMASK) + part * 4;
+        const int *src = (pc < 8 ? a.idx : vbits) + e0;
+        if (e0 + 4 <= nnz) {
+          cp_async16(dst, src);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) dst[i] = e0 + i < nnz ? __ldg(src + i) : 0;
+        }
+      }
+    };
+    auto issue = [&](int g) {
+      const int4 c = *reinterpret_cast<const int4 *>(sidx + ((4 * g) & SMASK));
+      float4 *slot = ring + ((4 * g) & (D - 1)) * 32 + lane;
+      cp_async16(slot, Bl + (uint64_t)((uint32_t)c.x & 0x7fffffffu) * ldb_bytes);
+      cp_async16(slot + 32, Bl + (uint64_t)((uint32_t)c.y & 0x7fffffffu) * ldb_bytes);
+      cp_async16(slot + 64, Bl + (uint64_t)((uint32_t)c.z & 0x7fffffffu) * ldb_bytes);
+      cp_async16(slot + 96, Bl + (uint64_t)((uint32_t)c.w & 0x7fffffffu) * ldb_bytes);
+    };
+    // the ring holds NCH chunks: the current one and the NCH - 1 after it
+    const int k0 = g0 >> 3;
+#pragma unroll 1
+    for (int k = k0; k < k0 + NCH; ++k)
+      if (32 * k < 4 * g1) stage(k);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp(sgmask);
+#pragma unroll 1
+    for (int i = 0; i < LAG; ++i) {
+      if (g0 + i < g1) issue(g0 + i);
+      cp_async_commit();
+    }
+#pragma unroll 1
+    for (int g = g0; g < g1; ++g) {
+      cp_async_wait<LAG - 1>();
+      if ((g & 7) == (LAG & 7)) __syncwarp(sgmask);  // the chunk staged LAG groups ago
+      const int x0 = 4 * g;
+      const int4 c = *reinterpret_cast<const int4 *>(sidx + (x0 & SMASK));
+      const float4 wv = *reinterpret_cast<const float4 *>(sval + (x0 & SMASK));
+      const float4 *slot = ring + (x0 & (D - 1)) * 32 + lane;
+      const float4 b0 = slot[0], b1 = slot[32], b2 = slot[64], b3 = slot[96];
+      if ((c.x | c.y | c.z | c.w) < 0) {
+        if (c.x < 0) { while (x0 == pe) finish_and_advance(); }
+        accumulate(wv.x, b0);
+        if (c.y < 0) { while (x0 + 1 == pe) finish_and_advance(); }
+        accumulate(wv.y, b1);
+        if (c.z < 0) { while (x0 + 2 == pe) finish_and_advance(); }
+        accumulate(wv.z, b2);
+        if (c.w < 0) { while (x0 + 3 == pe) finish_and_advance(); }
+        accumulate(wv.w, b3);
+      } else {
+        accumulate(wv.x, b0);
+        accumulate(wv.y, b1);
+        accumulate(wv.z, b2);
+        accumulate(wv.w, b3);
+      }
+      if ((g & 7) == 0 && g != g0) {
+        const int k = (g >> 3) + NCH - 1;  // into the slot of chunk (g >> 3) - 1, now consumed
+        if (32 * k < 4 * g1) {
+          __syncwarp(sgmask);  // the slots being refilled were read by every lane
+          stage(k);
+        }
+      }
+      if (g + LAG < g1) issue(g + LAG);
+      cp_async_commit();
+    }
+    cp_async_wait<0>();
+    for (int x = 4 * g1; x < pn; ++x) single(x);
+  }
+  while (cur < hdr.y) finish_and_advance();
+  if (hdr.w >= 0) {
+    float *dst = static_cast<float *>(a.scratch) + (int64_t)((hdr.z >= 0 && hdr.x == hdr.y) ? 2 * t : 2 * t + 1) * a.N + sl * 4;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) __stcg(dst + e, acc[e]);
+  }
+  if (hdr.z >= 0 && hdr.x < hdr.y) arrive<float, float, 4, SG, 1>(a, hdr.z, sl, sgmask);
+  if (hdr.w >= 0) arrive<float, float, 4, SG, 1>(a, hdr.w, sl, sgmask);
+}
+
 // ---------------------------------------------------------------- backward walks
 // One pass over A in row order for any of: Y = A X (DOY); dA_e = dY[row_e] . X[col_e] (DODA);
 // and, for A == A^T with equal values, dX = A^T dY = A dY (DODX: dY rows are gathered like
@@ -862,6 +1044,20 @@ swift_status launch_flag(MergeArgs a, const int *eidx, cudaStream_t st) {
   return SWIFT_OK;
 }
 
+template <int SG, int D>
+swift_status launch_staged(MergeArgs a, const int *eidx, cudaStream_t st) {
+  constexpr int G = 32 / SG;
+  constexpr int SMEM = staged_smem(SG, D);
+  const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
+  if (warps == 0) return SWIFT_OK;
+  a.idx = eidx;
+  auto k = merge_staged_kernel<SG, D, staged_minb(SG, D)>;
+  SW_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+  k<<<(unsigned)((warps + 7) / 8), 256, SMEM, st>>>(a);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
 template <class T, class TA, class ACC, int VB, int SG, int UNR, int MINB>
 swift_status launch_lean(const MergeArgs &a, cudaStream_t st) {
   constexpr int G = 32 / SG;
@@ -880,6 +1076,19 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   constexpr int V = VecWidth<T>::value;
   constexpr int W = WideWidth<T>::value;
   constexpr int AB = (int)sizeof(ACC);
+  // staged walk (kernel 4): FP32 values, B and C, one 16-byte slice per lane covering N;
+  // unr selects the ring depth (16 slots = 3 groups of 4 rows in flight, or 32 = 7 groups)
+  if constexpr (sizeof(T) == 4 && sizeof(TA) == 4 && sizeof(ACC) == 4) {
+    if (kernel == 4 && VB == V && VPL == 1 && a.N == SG * V && a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32) &&
+        (uintptr_t)eidx % 16 == 0 && (uintptr_t)a.val % 16 == 0) {
+      const bool deep = unr >= 16;
+      switch (SG) {
+        case 8: return deep ? launch_staged<8, 32>(a, eidx, st) : launch_staged<8, 16>(a, eidx, st);
+        case 16: return deep ? launch_staged<16, 32>(a, eidx, st) : launch_staged<16, 16>(a, eidx, st);
+        case 32: return deep ? launch_staged<32, 32>(a, eidx, st) : launch_staged<32, 16>(a, eidx, st);
+      }
+    }
+  }
   // flagged-index kernel (FP32-valued plans): 4 loads in flight
   // (FP64 values double the staging; 2-lane sub-warps would exceed 48 KB of static shared memory)
 #define SW_MCASE_FLAG(VB_, SG_)                                                                 \

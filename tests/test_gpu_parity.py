@@ -138,8 +138,8 @@ def test_long_row_split_is_deterministic(split):
 
 @pytest.mark.parametrize("U", [7, 32, 128, 256, 1024])
 @pytest.mark.parametrize("unr,vb,kern", [(4, 0, 1), (8, 0, 1), (4, 16, 2), (4, 32, 2), (16, 16, 3),
-                                         (8, 32, 3), (4, 4, 0)])
-@pytest.mark.parametrize("N", [4, 8, 33, 64, 128, 300, 512])
+                                         (8, 32, 3), (4, 4, 0), (8, 16, 4), (16, 16, 4)])
+@pytest.mark.parametrize("N", [4, 8, 32, 33, 64, 128, 300, 512])
 def test_row_engine_parameters(U, unr, vb, kern, N):
     """Every task size, load depth, vector width and kernel variant gives the same
     (deterministic) product; rows split across tasks are combined in task order."""
