@@ -208,7 +208,7 @@ def profile_summary(workload):
                 if ":" in line and not line.startswith(" "):
                     k, v = line.split(":", 1)
                     d[k.strip()] = v.strip()
-        if "dram_bytes_per_launch" in d and "kernel" in d:
+        if "dram_bytes_per_launch" in d and "kernel" in d and d.get("workload", "").split(" ")[0] == workload:
             d["file"] = os.path.relpath(path, ROOT)
             return d
     return {}
@@ -729,6 +729,20 @@ def run_ours(args):
     e2e_ms = t0.elapsed_time(t1)
     e2e_ms = max_over_ranks(e2e_ms, dist)
     e2e_value = world * flops * args.e2e_steps / (e2e_ms / 1e3) / 1e9
+    # the copy bound of that loop: one step's B in and C out on the same two streams, no product
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    c0.record(s_in)
+    s_out.wait_event(c0)
+    for i in range(2):
+        with torch.cuda.stream(s_in):
+            Bd[i % 2].copy_(Bh[i % 2], non_blocking=True)
+        with torch.cuda.stream(s_out):
+            Ch[i % 2].copy_(Cd[i % 2], non_blocking=True)
+    s_out.wait_stream(s_in)
+    c1.record(s_out)
+    torch.cuda.synchronize()
+    copy_ms = c0.elapsed_time(c1) / 2
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -773,7 +787,9 @@ def run_ours(args):
                 "h2d_bytes_per_step": int(Bh[0].numel() * Bh[0].element_size()),
                 "d2h_bytes_per_step": int(Ch[0].numel() * Ch[0].element_size()), "steps": args.e2e_steps,
                 "ms_per_step": e2e_ms / args.e2e_steps,
-                "pipeline": "H2D / product / D2H on three streams, two buffer sets"},
+                "pipeline": "H2D / product / D2H on three streams, two buffer sets",
+                "copy_bound_ms_per_step": copy_ms,
+                "frac_of_copy_bound": copy_ms / (e2e_ms / args.e2e_steps)},
         "gpu_launches": args.steps * (1 if engine == "rowwise" else 2),
         "clocks": clocks,
         "cpu_baseline": cpu,

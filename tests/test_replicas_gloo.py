@@ -57,3 +57,23 @@ def test_single_process_needs_no_group():
     import bench
     assert bench.max_over_ranks(3.5, None) == 3.5
     assert bench.whole_job_rate(10.0, 1, 2.0) == 5.0
+
+
+def test_profile_summaries_map_to_their_own_workload():
+    """Each committed ncu summary is found for its own workload only (a workload name that ends
+    another one's must not pick up the other's DRAM traffic)."""
+    import glob
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    seen = 0
+    for path in glob.glob(os.path.join(root, "profiles", "*.txt")):
+        with open(path) as f:
+            wl = next((ln.split(":", 1)[1].split()[0] for ln in f if ln.startswith("workload:")), None)
+        if wl is None:
+            continue
+        seen += 1
+        assert wl in bench.WORKLOADS, wl
+        assert bench.profile_summary(wl)["file"] == os.path.relpath(path, root)
+    assert seen >= 2
