@@ -61,6 +61,7 @@ WORKLOADS = {
     "sddmm_rmat20_n32_f32": dict(kind="sddmm", scale=20, edges=16 << 20, N=32, dtype="f32"),
     "sddmm_rmat20_n128_f32": dict(kind="sddmm", scale=20, edges=16 << 20, N=128, dtype="f32"),
     "sddmm_rmat19_n128_f32": dict(kind="sddmm", scale=19, edges=8 << 20, N=128, dtype="f32"),
+    "sddmm_rmat19_n32_f32": dict(kind="sddmm", scale=19, edges=8 << 20, N=32, dtype="f32"),
     # the 4096 x 4096 parity workload (rows ~Poisson(16))
     "poisson4096_n32_f32": dict(kind="poisson", M=4096, K=4096, lam=16.0, N=32, dtype="f32"),
 }

@@ -1313,7 +1313,15 @@ swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_
   RowLayout &L = p.fwd;
   {
     std::lock_guard<std::mutex> g(p.mu);
-    SW_TRY(build_merge_tasks(L, L.merge_built ? L.merge_U : 512, st));
+    // tasks shared with the forward walk when it ran (its tuned size); otherwise the largest
+    // power of two up to 512 that still gives about three waves of 32 warps per SM
+    int U = L.merge_U;
+    if (!L.merge_built) {
+      const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * 3);
+      U = 64;
+      while (U < 512 && 2 * U <= want) U *= 2;
+    }
+    SW_TRY(build_merge_tasks(L, U, st));
     const size_t need = (size_t)2 * L.ntasks * (size_t)N * (dX ? 2 : 1) * esz;
     if ((Y || dX) && need > L.mscratch.bytes) SW_TRY(L.mscratch.alloc(need));
   }
