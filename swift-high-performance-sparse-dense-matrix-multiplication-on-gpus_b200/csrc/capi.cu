@@ -63,11 +63,27 @@ static size_t dtype_size(swift_dtype d) {
   return 0;
 }
 
+// Untuned row-walk parameters for layout L and dense width N: the default walk with tasks of
+// the largest power of two up to 512 positions that still leaves about `waves` waves of 32
+// warps per SM (narrow rows pack several tasks into a warp, so they want smaller tasks).
+// Measured best: six for A's rows, three for the rows of A^T.
+MergeOpts default_merge_opts(const Plan &p, const RowLayout &L, int N, swift_dtype dt, int waves) {
+  MergeOpts o;
+  const int esz = dt == SWIFT_F64 ? 8 : (dt == SWIFT_F32 ? 4 : 2);
+  const int lanes = std::max(1, (N * esz + 15) / 16);
+  int SG = 2;
+  while (SG < lanes && SG < 32) SG <<= 1;
+  const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * waves);
+  o.U = 64;
+  while (o.U < 512 && 2 * o.U <= want) o.U *= 2;
+  return o;
+}
+
 MergeOpts merge_opts_for(Plan &p, int N, swift_dtype dt) {
   std::lock_guard<std::mutex> g(p.mu);
   if (p.merge_override) return p.merge_opts;
   auto it = p.tuned_merge.find({N, (int)dt});
-  return it != p.tuned_merge.end() ? it->second : p.merge_opts;
+  return it != p.tuned_merge.end() ? it->second : default_merge_opts(p, p.fwd, N, dt, 6);
 }
 
 swift_status ensure_bwd(Plan &p, cudaStream_t st) {
@@ -303,7 +319,7 @@ swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dt
   if (p.K == 0 || N == 0) return SWIFT_OK;
   DenseArgs d;
   d.N = N; d.dtype = dtype; d.B = Y; d.ldb = ldy; d.C = X; d.ldc = ldx;
-  return run_merge(p, p.bwd, d, MergeOpts{}, st);
+  return run_merge(p, p.bwd, d, default_merge_opts(p, p.bwd, N, dtype, 3), st);
 }
 
 swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const void *U,
@@ -373,7 +389,7 @@ swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_d
     SW_TRY(ensure_bwd(p, st));
     DenseArgs d;
     d.N = N; d.dtype = dtype; d.B = dY; d.ldb = lddy; d.C = dX; d.ldc = lddx;
-    SW_TRY(run_merge(p, p.bwd, d, MergeOpts{}, st));
+    SW_TRY(run_merge(p, p.bwd, d, default_merge_opts(p, p.bwd, N, dtype, 3), st));
   }
   return SWIFT_OK;
 }

@@ -1314,10 +1314,10 @@ swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_
   {
     std::lock_guard<std::mutex> g(p.mu);
     // tasks shared with the forward walk when it ran (its tuned size); otherwise the largest
-    // power of two up to 512 that still gives about three waves of 32 warps per SM
+    // power of two up to 512 that still gives about six waves of 32 warps per SM
     int U = L.merge_U;
     if (!L.merge_built) {
-      const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * 3);
+      const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * 6);
       U = 64;
       while (U < 512 && 2 * U <= want) U *= 2;
     }
