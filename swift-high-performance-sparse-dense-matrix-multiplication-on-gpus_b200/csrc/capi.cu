@@ -32,7 +32,8 @@ size_t plan_device_bytes(const Plan &p) {
     const DevBuf *lb[] = {&L->piece_row, &L->piece_idx, &L->long_first, &L->long_count,
                           &L->long_of_row, &L->counters, &L->scratch, &L->task_row,
                           &L->head_split, &L->tail_split, &L->split_row, &L->split_first,
-                          &L->split_last, &L->split_cnt, &L->mscratch, &L->task_hdr, &L->eidx};
+                          &L->split_last, &L->split_cnt, &L->mscratch, &L->task_hdr, &L->eidx,
+                          &L->sdd_hdr};
     for (const DevBuf *b : lb) s += b->bytes;
   }
   return s;

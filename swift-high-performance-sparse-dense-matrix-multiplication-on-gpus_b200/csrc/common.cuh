@@ -131,6 +131,9 @@ struct RowLayout {
   DevBuf eidx;                        // [nnz] gather indices, bit 31 set on each row's first
   DevBuf split_row, split_first, split_last, split_cnt;  // [nsplit]
   DevBuf mscratch;                    // [2*ntasks][N] partial rows ([2*ntasks][2N] for [Y | dX])
+  // SDDMM alone needs no split-row bookkeeping, so it walks its own finer tasks
+  int sdd_U = 0, sdd_ntasks = 0;
+  DevBuf sdd_hdr;                     // [sdd_ntasks] int4 (first row, last row, -1, -1)
 };
 
 // Parameters of the merge-path row engine (autotuned per (N, dtype); overridable).

@@ -904,6 +904,12 @@ __global__ void task_hdr_kernel(const int *__restrict__ task_row, const int *__r
     hdr[t] = make_int4(task_row[t], task_row[t + 1], hs[t], ts[t]);
 }
 
+__global__ void sdd_hdr_kernel(const int *__restrict__ task_row, int ntasks, int4 *__restrict__ hdr) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks;
+       t += (int64_t)gridDim.x * blockDim.x)
+    hdr[t] = make_int4(task_row[t], task_row[t + 1], -1, -1);
+}
+
 // task_row[t] = smallest row whose span reaches position t*U (rows for t = ntasks).
 __global__ void task_row_kernel(const int *__restrict__ ptr, int rows, int64_t total, int U,
                                 int ntasks, int *__restrict__ task_row) {
@@ -1311,19 +1317,40 @@ swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_
   int SG = 4;
   while (SG < lanes) SG <<= 1;
   RowLayout &L = p.fwd;
+  const bool sdd_only = !Y && !dX;
+  // largest power of two in [lo, 512] that leaves about `waves` waves of 32 warps per SM
+  auto wave_size = [&](int lo, int waves) {
+    const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * waves);
+    int U = lo;
+    while (U < 512 && 2 * U <= want) U *= 2;
+    return U;
+  };
+  int sdd_U = 0;
   {
     std::lock_guard<std::mutex> g(p.mu);
-    // tasks shared with the forward walk when it ran (its tuned size); otherwise the largest
-    // power of two up to 512 that still gives about six waves of 32 warps per SM
-    int U = L.merge_U;
-    if (!L.merge_built) {
-      const int64_t want = ((int64_t)L.nnz + L.rows) / ((int64_t)p.sm_count * 32 * (32 / SG) * 6);
-      U = 64;
-      while (U < 512 && 2 * U <= want) U *= 2;
-    }
-    SW_TRY(build_merge_tasks(L, U, st));
+    // tasks shared with the forward walk when it ran (its tuned size), else about six waves
+    SW_TRY(build_merge_tasks(L, L.merge_built ? L.merge_U : wave_size(64, 6), st));
     const size_t need = (size_t)2 * L.ntasks * (size_t)N * (dX ? 2 : 1) * esz;
     if ((Y || dX) && need > L.mscratch.bytes) SW_TRY(L.mscratch.alloc(need));
+    if (sdd_only) {
+      // SDDMM alone: no partial rows to combine, so many small tasks cost nothing extra and
+      // shorten the tail (measured best near 24 waves: 32 positions at N=32, 128 at N=128)
+      sdd_U = wave_size(32, 24);
+      if (L.sdd_U != sdd_U || !L.sdd_hdr.p) {
+        const int64_t total = (int64_t)L.nnz + L.rows;
+        const int64_t nt = (total + sdd_U - 1) / sdd_U;
+        if (nt >= INT32_MAX / 2) return SWIFT_ERR_OVERFLOW;
+        TmpBuf tr;
+        SW_TRY(tr.alloc(sizeof(int) * ((size_t)nt + 1), st));
+        task_row_kernel<<<grid_n(nt + 1), 256, 0, st>>>(L.ptr, L.rows, total, sdd_U, (int)nt, tr.as<int>());
+        SW_CHECK_LAUNCH();
+        SW_TRY(L.sdd_hdr.alloc(sizeof(int4) * (size_t)std::max<int64_t>(nt, 1)));
+        if (nt > 0) sdd_hdr_kernel<<<grid_n(nt), 256, 0, st>>>(tr.as<int>(), (int)nt, L.sdd_hdr.as<int4>());
+        SW_CHECK_LAUNCH();
+        L.sdd_U = sdd_U;
+        L.sdd_ntasks = (int)nt;
+      }
+    }
   }
   BwdArgs ba{};
   MergeArgs &a = ba.m;
@@ -1336,6 +1363,11 @@ swift_status run_bwd_merge(Plan &p, int N, swift_dtype dt, const void *X, int64_
   a.split_row = L.split_row.as<int>(); a.split_first = L.split_first.as<int>();
   a.split_last = L.split_last.as<int>(); a.split_cnt = L.split_cnt.as<int>();
   a.scratch = L.mscratch.p;
+  if (sdd_only) {
+    a.U = sdd_U;
+    a.ntasks = L.sdd_ntasks;
+    a.task_hdr = L.sdd_hdr.as<int>();
+  }
   ba.dY = dY; ba.lddy = lddy; ba.dX = dX; ba.lddx = lddx; ba.dA = dA;
   const bool y = Y != nullptr, da = dA != nullptr, dx = dX != nullptr;
   return dt == SWIFT_F64 ? bwd_dispatch<double>(ba, VB, SG, y, da, dx, st)
