@@ -268,16 +268,6 @@ swift_status launch_colmajor(const TiledArgs &a, cudaStream_t st) {
   return SWIFT_OK;
 }
 
-__global__ void zero_rows_kernel(char *C, int rows, size_t row_bytes, int64_t pitch) {
-  // row_bytes and pitch are multiples of 4
-  const int64_t words = (int64_t)(row_bytes / 4);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)rows * words;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = i / words, w = i - r * words;
-    reinterpret_cast<int *>(C + r * pitch)[w] = 0;
-  }
-}
-
 }  // namespace
 
 swift_status zero_dense(void *C, int rows, int N, int64_t ld, swift_layout layout, size_t esz,
