@@ -80,7 +80,8 @@ typedef enum swift_memspace { SWIFT_HOST = 0, SWIFT_DEVICE = 1 } swift_memspace;
  *              atomic into C, plus the load-balanced reside blocks.  Any layout of B and C.
  *   ROWWISE -- row-ordered execution for C much larger than L2: each C row is accumulated
  *              in registers and written once; rows longer than the split threshold are cut
- *              into pieces combined deterministically.  Row-major B and C.
+ *              into pieces combined deterministically.  Column-major B or C are transposed
+ *              into row-major copies held by the plan (not with b_presorted).
  *   AUTO    -- the autotuned choice for (N, dtype), ROWWISE when no tuning was run and the
  *              layouts allow it. */
 typedef enum swift_engine { SWIFT_ENGINE_AUTO = 0, SWIFT_ENGINE_TILED = 1, SWIFT_ENGINE_ROWWISE = 2 } swift_engine;

@@ -25,7 +25,7 @@ size_t plan_device_bytes(const Plan &p) {
                           &p.step_tall, &p.step_tile_off, &p.item_tile, &p.tile_colidx,
                           &p.tile_depth, &p.tile_tall, &p.tile_format, &p.sortrowidx, &p.sortval,
                           &p.reside_ptr, &p.reside_row, &p.reside_val, &p.colorblk, &p.blkstart,
-                          &p.blkstop, &p.blkptr};
+                          &p.blkstop, &p.blkptr, &p.rowcopy_b, &p.rowcopy_c};
   size_t s = 0;
   for (const DevBuf *b : bufs) s += b->bytes;
   for (const RowLayout *L : {&p.fwd, &p.bwd}) {
@@ -293,6 +293,39 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
   d.C = C; d.ldc = ldc; d.c_layout = c_layout;
   cudaStream_t st = S(stream);
   const bool row_ok = p.has_csr && b_layout == SWIFT_ROW_MAJOR && c_layout == SWIFT_ROW_MAJOR && !b_presorted;
+  // Column-major operands: in that layout each nonzero's N contributions land M elements apart,
+  // so the row walk runs on row-major copies instead (B transposed in, C transposed out through
+  // plan-held buffers, like the plan's other scratch); the tiled engine keeps the direct
+  // column-major kernel.
+  const bool via_rows = p.has_csr && !b_presorted && !row_ok && p.M > 0 && N > 0 &&
+                        (engine == SWIFT_ENGINE_ROWWISE || (engine == SWIFT_ENGINE_AUTO && [&] {
+                           std::lock_guard<std::mutex> g(p.mu);
+                           auto it = p.tuned.find({N, (int)dtype});
+                           return it == p.tuned.end() || it->second == SWIFT_ENGINE_ROWWISE;
+                         }()));
+  if (via_rows) {
+    const size_t esz = dtype == SWIFT_F64 ? 8 : (dtype == SWIFT_F32 ? 4 : 2);
+    DenseArgs r = d;
+    r.b_layout = r.c_layout = SWIFT_ROW_MAJOR;
+    {
+      std::lock_guard<std::mutex> g(p.mu);
+      const size_t nb = esz * (size_t)p.K * N, nc = esz * (size_t)p.M * N;
+      if (b_layout == SWIFT_COL_MAJOR && p.rowcopy_b.bytes < nb) SW_TRY(p.rowcopy_b.alloc(nb));
+      if (c_layout == SWIFT_COL_MAJOR && p.rowcopy_c.bytes < nc) SW_TRY(p.rowcopy_c.alloc(nc));
+    }
+    if (b_layout == SWIFT_COL_MAJOR) {
+      SW_TRY(transpose_dense(B, p.K, N, ldb, p.rowcopy_b.p, N, esz, st));
+      r.B = p.rowcopy_b.p;
+      r.ldb = N;
+    }
+    if (c_layout == SWIFT_COL_MAJOR) {
+      r.C = p.rowcopy_c.p;
+      r.ldc = N;
+    }
+    SW_TRY(run_merge(p, p.fwd, r, merge_opts_for(p, N, dtype), st));
+    if (c_layout == SWIFT_COL_MAJOR) SW_TRY(transpose_dense(p.rowcopy_c.p, N, p.M, N, C, ldc, esz, st));
+    return SWIFT_OK;
+  }
   if (engine == SWIFT_ENGINE_AUTO) {
     engine = row_ok ? SWIFT_ENGINE_ROWWISE : SWIFT_ENGINE_TILED;
     std::lock_guard<std::mutex> g(p.mu);

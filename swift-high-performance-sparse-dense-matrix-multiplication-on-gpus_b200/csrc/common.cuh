@@ -195,6 +195,8 @@ struct Plan {
   // backward then computes dX = A dY in the same pass.  use_symmetry = 0 disables that.
   int symmetric = -1;
   int use_symmetry = 1;
+  // row-major copies of column-major dense operands for the row walk (grown on demand)
+  DevBuf rowcopy_b, rowcopy_c;
   std::mutex mu;  // guards lazily built layouts and scratch growth
 };
 
@@ -210,6 +212,10 @@ swift_status radix_sort_pairs(uint32_t *keys_in, uint32_t *vals_in, uint32_t *ke
                               uint32_t *vals_out, int64_t n, int bits, cudaStream_t st);
 // max over n int32 (n >= 0) into *dev_out (single int on device)
 swift_status reduce_max_i32(const int *in, int64_t n, int *dev_out, cudaStream_t st);
+// out[r * ld_out + c] = in[r + c * ld_in] for r < rows, c < cols: a column-major matrix
+// rewritten row-major (with rows and cols swapped, the reverse).  esz = 2, 4 or 8 bytes.
+swift_status transpose_dense(const void *in, int rows, int cols, int64_t ld_in, void *out,
+                             int64_t ld_out, size_t esz, cudaStream_t st);
 
 // ---------------------------------------------------------------- format build (format_build.cu)
 swift_status build_from_csr(Plan &p, const swift_csr &A, const swift_plan_opts *opts,

@@ -77,42 +77,6 @@ int grid_warps(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, 148 * 32));
 }
 
-// out[r * cols + c] = in[r + c * rows]: a column-major rows x cols matrix (leading dimension
-// rows) rewritten row-major.  The same call with rows and cols swapped turns a row-major matrix
-// back into column-major.  32 x 32 tiles pass through shared memory (one padding column keeps
-// the transposed reads on distinct banks) so that both the loads and the stores of a warp cover
-// 32 consecutive elements; blocks walk the tiles down the input's columns.
-template <class T>
-__global__ void __launch_bounds__(256) transpose_kernel(const T *__restrict__ in, int rows, int cols,
-                                                        T *__restrict__ out) {
-  __shared__ T tile[32][33];
-  const int64_t ntr = (rows + 31) / 32, ntiles = ntr * ((cols + 31) / 32);
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t r0 = (t % ntr) * 32, c0 = (t / ntr) * 32;
-    for (int j = ty; j < 32; j += 8) {
-      const int64_t r = r0 + tx, c = c0 + j;
-      if (r < rows && c < cols) tile[j][tx] = in[r + c * rows];
-    }
-    __syncthreads();
-    for (int j = ty; j < 32; j += 8) {
-      const int64_t r = r0 + j, c = c0 + tx;
-      if (r < rows && c < cols) out[r * cols + c] = tile[tx][j];
-    }
-    __syncthreads();
-  }
-}
-
-template <class T>
-swift_status transpose(const void *in, int rows, int cols, void *out, cudaStream_t st) {
-  const int64_t ntiles = ((int64_t)rows + 31) / 32 * (((int64_t)cols + 31) / 32);
-  if (ntiles == 0) return SWIFT_OK;
-  const int grid = (int)std::min<int64_t>(ntiles, 148 * 8);
-  transpose_kernel<T><<<grid, 256, 0, st>>>(static_cast<const T *>(in), rows, cols, static_cast<T *>(out));
-  SW_CHECK_LAUNCH();
-  return SWIFT_OK;
-}
-
 template <class T> swift_status upload(DevBuf &d, const T *h, size_t n, cudaStream_t st) {
   SW_TRY(d.alloc(sizeof(T) * n));
   if (n) SW_CHECK_CUDA(cudaMemcpyAsync(d.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
@@ -487,9 +451,9 @@ swift_status ref_spmm(int variant, const SLIDE *m, int rowA, int colA, int width
   d.b_layout = d.c_layout = SWIFT_ROW_MAJOR;
   d.ldb = d.ldc = std::max(width, 1);
   Timer tm(st);
-  if (colmajor) SW_TRY(transpose<T>(B.p, colA, width, Bt.p, st));
+  if (colmajor) SW_TRY(transpose_dense(B.p, colA, width, colA, Bt.p, width, sizeof(T), st));
   SW_TRY(run_tiled(p, d, variant == 1 ? 1 : 0, st));
-  if (colmajor) SW_TRY(transpose<T>(Ct.p, width, rowA, C.p, st));
+  if (colmajor) SW_TRY(transpose_dense(Ct.p, width, rowA, width, C.p, rowA, sizeof(T), st));
   const float t = tm.stop();
   if (ms) *ms = t;
   SW_TRY(download(h_C, C.p, (size_t)rowA * width, st));

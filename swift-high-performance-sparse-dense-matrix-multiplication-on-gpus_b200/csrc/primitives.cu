@@ -247,6 +247,67 @@ swift_status radix_sort_pairs(uint32_t *keys_in, uint32_t *vals_in, uint32_t *ke
   return SWIFT_OK;
 }
 
+namespace {
+// Tiles of 32 * TR rows x 32 columns through shared memory (one padding element per tile row
+// keeps the transposed reads on distinct banks), so both a warp's loads and its stores cover
+// 32 consecutive elements and each thread keeps 4 * TR loads in flight; blocks walk the tiles
+// down the input's columns.
+template <class E, int TR>
+__global__ void __launch_bounds__(256) transpose_kernel(const E *__restrict__ in, int rows, int cols,
+                                                        int64_t ld_in, E *__restrict__ out, int64_t ld_out) {
+  constexpr int R = 32 * TR;
+  __shared__ E tile[32][R + 1];
+  const int64_t ntr = (rows + R - 1) / R, ntiles = ntr * ((cols + 31) / 32);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t r0 = (t % ntr) * R, c0 = (t / ntr) * 32;
+#pragma unroll
+    for (int j = ty; j < 32; j += 8) {
+#pragma unroll
+      for (int q = 0; q < TR; ++q) {
+        const int64_t r = r0 + 32 * q + tx, c = c0 + j;
+        if (r < rows && c < cols) tile[j][32 * q + tx] = in[r + c * ld_in];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = ty; j < R; j += 8) {
+      const int64_t r = r0 + j, c = c0 + tx;
+      if (r < rows && c < cols) out[r * ld_out + c] = tile[tx][j];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+swift_status transpose_dense(const void *in, int rows, int cols, int64_t ld_in, void *out,
+                             int64_t ld_out, size_t esz, cudaStream_t st) {
+  const int64_t ntiles = ((int64_t)rows + 31) / 32 * (((int64_t)cols + 31) / 32);
+  if (ntiles == 0) return SWIFT_OK;
+  constexpr int TR = 4;
+  const int64_t ntiles4 = ((int64_t)rows + 32 * TR - 1) / (32 * TR) * (((int64_t)cols + 31) / 32);
+  const int grid = (int)std::min<int64_t>(ntiles4, 148 * 8);
+  switch (esz) {
+    case 2:
+      transpose_kernel<uint16_t, TR><<<grid, 256, 0, st>>>(static_cast<const uint16_t *>(in), rows, cols, ld_in,
+                                                           static_cast<uint16_t *>(out), ld_out);
+      break;
+    case 4:
+      transpose_kernel<uint32_t, TR><<<grid, 256, 0, st>>>(static_cast<const uint32_t *>(in), rows, cols, ld_in,
+                                                           static_cast<uint32_t *>(out), ld_out);
+      break;
+    case 8:
+      transpose_kernel<uint64_t, TR><<<grid, 256, 0, st>>>(static_cast<const uint64_t *>(in), rows, cols, ld_in,
+                                                           static_cast<uint64_t *>(out), ld_out);
+      break;
+    default:
+      return SWIFT_ERR_UNSUPPORTED;
+  }
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
 swift_status reduce_max_i32(const int *in, int64_t n, int *dev_out, cudaStream_t st) {
   SW_CHECK_CUDA(cudaMemsetAsync(dev_out, 0, sizeof(int), st));
   if (n <= 0) return SWIFT_OK;

@@ -99,6 +99,32 @@ def test_tiled_colmajor_presorted_like_reference_wrappers(name, dt):
     pl.close()
 
 
+@pytest.mark.parametrize("dt", ["f32", "f64", "bf16"])
+@pytest.mark.parametrize("engine", ["auto", "rowwise"])
+@pytest.mark.parametrize("N", [32, 33, 128])
+@pytest.mark.parametrize("pad", [0, 5])
+def test_column_major_operands_through_the_row_walk(dt, engine, N, pad):
+    """Column-major B and C (leading dimensions exact or padded) run the row walk on row-major
+    copies: the same bits as the row-major product, padding untouched."""
+    M, K, rp, ci = cases.make("rmat12", 0)
+    npdt = np.float64 if dt == "f64" else np.float32
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[dt]
+    val = gen.uniform_values(int(rp[-1]), 1, npdt)
+    B = tdev(gen.dense_uniform(K, N, 2, npdt)).to(tdt)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    Crow = pl.spmm(B, engine="rowwise")
+    Bbig = torch.zeros((N, K + pad), dtype=tdt, device="cuda")
+    Bbig[:, :K] = B.t()
+    Cbig = torch.full((N, M + (3 if pad else 0)), 7.0, dtype=tdt, device="cuda")
+    Ccm = Cbig[:, :M].t()
+    pl.spmm(Bbig[:, :K].t(), C_out=Ccm, engine=engine, layout="col")
+    assert torch.equal(Ccm, Crow)
+    assert bool((Cbig[:, M:] == 7.0).all())
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, B.double().cpu().numpy())
+    assert relerr(Ccm.double().cpu().numpy(), ref) <= (1e-2 if dt == "bf16" else TOL[npdt])
+    pl.close()
+
+
 @pytest.mark.parametrize("N", [1, 8, 24, 32, 33, 64, 128, 768])
 @pytest.mark.parametrize("engine", ["tiled", "rowwise"])
 def test_ragged_widths(N, engine):
