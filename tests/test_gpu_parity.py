@@ -125,6 +125,22 @@ def test_column_major_operands_through_the_row_walk(dt, engine, N, pad):
     pl.close()
 
 
+@pytest.mark.parametrize("name", cases.SMALL)
+@pytest.mark.parametrize("N", [4, 33])
+def test_column_major_small_and_edge_shapes(name, N):
+    """Column-major operands through the row walk on every small / edge shape (empty matrix,
+    K < 32, rectangular, long columns): equal to the row-major product."""
+    M, K, rp, ci = cases.make(name, 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    B = tdev(gen.dense_uniform(K, N, 2, np.float32))
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    Crow = pl.spmm(B, engine="rowwise")
+    Ccm = pl.spmm(B.t().contiguous().t(), engine="auto", layout="col")
+    assert Ccm.stride(0) == 1 and torch.equal(Ccm, Crow)
+    assert relerr(Ccm.cpu().numpy(), oracle.csr_spmm_f64(M, K, rp, ci, val, B.cpu().numpy())) <= 1e-5
+    pl.close()
+
+
 @pytest.mark.parametrize("N", [1, 8, 24, 32, 33, 64, 128, 768])
 @pytest.mark.parametrize("engine", ["tiled", "rowwise"])
 def test_ragged_widths(N, engine):
