@@ -665,7 +665,12 @@ def run_ours(args):
     d_ci = torch.from_numpy(ci).cuda()
     plan = Plan.from_csr(d_rp, d_ci, val, (M, K))
     C = torch.empty((M, N), dtype=B.dtype, device="cuda")
-    engine, tune_ms = plan.autotune(B, C)
+    if args.rowwise_params:
+        U, unr, vb, kern = (int(x) for x in args.rowwise_params.split(","))
+        plan.set_rowwise_params(U, unr, vb, kern)
+        engine, tune_ms = "rowwise", 0.0
+    else:
+        engine, tune_ms = plan.autotune(B, C)
     rw_params = plan.rowwise_params(N, B.dtype) if engine == "rowwise" else None
     st = plan.stats()
     stream = torch.cuda.current_stream()
@@ -1052,6 +1057,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rowwise-params", help="task_size,loads_in_flight,vector_bytes,kernel: run the row "
+                                             "engine with these instead of autotuning (e.g. for a profile)")
     ap.add_argument("--mtx", help="MatrixMarket coordinate file: run the product on this matrix instead "
                                   "of a synthetic workload")
     ap.add_argument("--n", type=int, default=128, help="dense columns with --mtx")
