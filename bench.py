@@ -346,6 +346,22 @@ def run_precision(args):
         res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": eng,
                      "err_vs_fp64": err, "err_vs_fp64_on_rounded_B": err_in,
                      "algorithmic_bytes": bytes_, "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / hbm_peak()[0]}
+    # 16-bit B and C with per-row power-of-two scales (swift_spmm_scaled): B rows stored as
+    # B / b_scale with each row's maximum in [2^14, 2^15); error of c_scale * C against FP64
+    m = B32.abs().amax(dim=1)
+    bscale = torch.where(m > 0, torch.exp2(torch.floor(torch.log2(torch.where(m > 0, m, torch.ones_like(m)))) - 14),
+                         torch.ones_like(m)).float().contiguous()
+    for name, dt in (("bf16_scaled", torch.bfloat16), ("f16_scaled", torch.float16)):
+        B = (B32 / bscale[:, None]).to(dt)
+        C = torch.empty((M, N), dtype=dt, device="cuda")
+        cs = torch.empty(M, dtype=torch.float32, device="cuda")
+        ms = _timed(lambda: plan.spmm_scaled(B, b_scale=bscale, C_out=C, c_scale=cs), args.steps, args.warmup)
+        plan.spmm_scaled(B, b_scale=bscale, C_out=C, c_scale=cs)
+        err = (C.double() * cs.double()[:, None] - ref).abs().max().item() / refmax
+        bytes_ = nnz * 8 + (K + M) * (N * B.element_size() + 4)
+        res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": "rowwise",
+                     "err_vs_fp64": err, "algorithmic_bytes": bytes_,
+                     "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / hbm_peak()[0]}
     f32b, bfb = res["f32"]["algorithmic_bytes"], res["bf16"]["algorithmic_bytes"]
     out = {
         "metric": "spmm_gflops", "value": res["bf16"]["gflops"], "unit": "GFLOP/s", "n_gpus": 1,

@@ -213,6 +213,20 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
                         const void *B, int64_t ldb, swift_layout b_layout, int b_presorted,
                         void *C, int64_t ldc, swift_layout c_layout, swift_stream_t stream);
 
+/* C = A * B with 16-bit operands scaled per row, for values outside FP16's range (or that
+ * would lose BF16's few mantissa bits near its extremes).  dtype BF16 or F16, F32 plan;
+ * row-major B (K x N, rows in A's column order) and C (M x N).  Row k of B holds
+ * B_true[k] / b_scale[k] (b_scale: K floats on the device, or NULL for all 1); each product
+ * term is A[r][k] * b_scale[k] * B[k][n], accumulated in F32.  C row r is written as
+ * C_true[r] / c_scale[r] with c_scale[r] (M floats on the device) the power of two that
+ * puts the row's largest magnitude in [2^14, 2^15) (1 for an all-zero row), so the 16-bit
+ * rows neither overflow nor flush to zero.  Row walk only, N <= 256, B / C / ldb / ldc
+ * 16-byte aligned; other shapes return SWIFT_ERR_UNSUPPORTED.  No counterpart in the
+ * reference (FP32 / FP64 only). */
+swift_status swift_spmm_scaled(const swift_plan *plan, int N, swift_dtype dtype, const void *B, int64_t ldb,
+                               const float *b_scale, void *C, int64_t ldc, float *c_scale,
+                               swift_stream_t stream);
+
 /* X = A^T * Y (row-major, K x N and M x N): the backward product dX = A^T dY. */
 swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dtype,
                                    const void *Y, int64_t ldy, void *X, int64_t ldx,

@@ -341,6 +341,23 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
   return SWIFT_ERR_INVALID_ARG;
 }
 
+swift_status swift_spmm_scaled(const swift_plan *plan, int N, swift_dtype dtype, const void *B, int64_t ldb,
+                               const float *b_scale, void *C, int64_t ldc, float *c_scale,
+                               swift_stream_t stream) {
+  SW_TRY(check_dense(plan, N, dtype, B, ldb, SWIFT_ROW_MAJOR, plan ? plan->p.K : 0, C, ldc, SWIFT_ROW_MAJOR,
+                     plan ? plan->p.M : 0));
+  if (dtype != SWIFT_BF16 && dtype != SWIFT_F16) return SWIFT_ERR_UNSUPPORTED;
+  Plan &p = const_cast<Plan &>(plan->p);
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  if (N == 0 || p.M == 0) return SWIFT_OK;
+  if (!c_scale) return SWIFT_ERR_INVALID_ARG;
+  DenseArgs d;
+  d.N = N; d.dtype = dtype; d.B = B; d.ldb = ldb; d.C = C; d.ldc = ldc;
+  d.b_scale = b_scale;
+  d.c_scale = c_scale;
+  return run_merge(p, p.fwd, d, merge_opts_for(p, N, dtype), S(stream));
+}
+
 swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dtype,
                                    const void *Y, int64_t ldy, void *X, int64_t ldx,
                                    swift_stream_t stream) {

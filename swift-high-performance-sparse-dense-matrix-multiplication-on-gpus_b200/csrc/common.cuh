@@ -256,6 +256,11 @@ struct DenseArgs {
   void *C = nullptr;
   int64_t ldc = 0;
   swift_layout c_layout = SWIFT_ROW_MAJOR;
+  // 16-bit operands with per-row scales (row walk only): B row k holds B_true[k] / b_scale[k]
+  // (b_scale may be null: all 1); C row r is written as C_true[r] / c_scale[r], c_scale[r] a
+  // power of two chosen per row
+  const float *b_scale = nullptr;
+  float *c_scale = nullptr;
 };
 // variant 1 = reside per column without balance blocks (Swift_gpu1's kernel)
 swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cudaStream_t st);

@@ -36,6 +36,8 @@ struct MergeArgs {
   const int *split_row, *split_first, *split_last;
   int *split_cnt;
   void *scratch;  // [2 * ntasks][N] partial rows
+  const float *b_scale;  // per-B-row scales (scaled 16-bit walk): folded into the values
+  float *c_scale;        // per-C-row scales (scaled 16-bit walk): written with each row
 };
 
 namespace {
@@ -46,6 +48,34 @@ constexpr int unroll_for(int VB, int VPL, bool deep, int acc_bytes) {
   const int lim = 256 / (VB * VPL * acc_bytes) > 0 ? 256 / (VB * VPL * acc_bytes) : 1;
   const int base = deep ? 16 : 8;
   return base < lim ? base : lim;
+}
+
+// Per-row scale of 16-bit C: the power of two s that puts the row's largest magnitude m in
+// [2^14, 2^15) (well inside FP16's range and BF16's), 1 for an all-zero row.  Every lane of the
+// sub-warp returns the same s; dividing by a power of two is exact.
+template <int SG>
+__device__ __forceinline__ float row_scale(float m, unsigned sgmask) {
+#pragma unroll
+  for (int o = SG / 2; o >= 1; o >>= 1) m = fmaxf(m, __shfl_xor_sync(sgmask, m, o, SG));
+  if (!(m > 0.f) || !(m < 3.0e38f)) return 1.f;
+  const int e = (int)((__float_as_uint(m) >> 23) & 0xffu) - 127;  // floor(log2 m), normal m
+  const int se = min(max(e - 14, -126), 127);
+  return __uint_as_float((unsigned)(se + 127) << 23);
+}
+
+// Writes a finished row of the scaled walk: divided by its scale, which lane 0 records.
+template <class T, class ACC, int VB, int SG>
+__device__ __forceinline__ void store_scaled_row(const MergeArgs &a, int orow, int sl, unsigned sgmask,
+                                                 ACC (&acc)[VB], bool inb) {
+  float m = 0.f;
+#pragma unroll
+  for (int e = 0; e < VB; ++e) m = fmaxf(m, fabsf((float)acc[e]));
+  const float s = row_scale<SG>(m, sgmask);
+  const float inv = 1.f / s;  // exact: s is a power of two
+#pragma unroll
+  for (int e = 0; e < VB; ++e) acc[e] = (ACC)((float)acc[e] * inv);
+  if (sl == 0) a.c_scale[orow] = s;
+  if (inb) vstore<T, ACC, VB>(static_cast<T *>(a.C) + (int64_t)orow * a.ldc + sl * VB, acc);
 }
 
 template <class T, class ACC, int VB, int SG, int VPL>
@@ -70,7 +100,7 @@ __device__ __forceinline__ void store_partial(const MergeArgs &a, int slot, int 
 }
 
 // Counts this task's arrival for split row s; the last task adds the partials in task order.
-template <class T, class ACC, int VB, int SG, int VPL>
+template <class T, class ACC, int VB, int SG, int VPL, bool SCALE = false>
 __device__ __forceinline__ void arrive(const MergeArgs &a, int s, int sl, unsigned sgmask) {
   __threadfence();
   __syncwarp(sgmask);
@@ -97,7 +127,13 @@ __device__ __forceinline__ void arrive(const MergeArgs &a, int s, int sl, unsign
         for (int e = 0; e < VB; ++e)
           if (col0 + v * SG * VB + sl * VB + e < a.N) acc[v][e] += __ldcg(src + v * SG * VB + e);
     }
-    store_c<T, ACC, VB, SG, VPL>(a, a.split_row[s], col0, sl, acc);
+    if constexpr (SCALE) {  // the scaled walk's rows fit one chunk (N <= SG * VB, VPL == 1)
+      const int row = a.split_row[s];
+      store_scaled_row<T, ACC, VB, SG>(a, a.out_row ? __ldg(a.out_row + row) : row, sl, sgmask, acc[0],
+                                       col0 + sl * VB < a.N);
+    } else {
+      store_c<T, ACC, VB, SG, VPL>(a, a.split_row[s], col0, sl, acc);
+    }
   }
   __syncwarp(sgmask);
   if (sl == 0) a.split_cnt[s] = 0;  // ready for the next product
@@ -289,9 +325,12 @@ __global__ void __launch_bounds__(256, MINB) merge_lean_kernel(const MergeArgs a
 // with one broadcast load per nonzero; full chunks run fully unrolled.
 // One task of the flagged walk by one sub-warp (sl = lane within the sub-warp, stage = its
 // 32-entry staging buffer).
-template <class T, class TA, class ACC, int VB, int SG, bool FULL = false>
+// SCALE (16-bit B and C only): values multiplied by their column's b_scale as they are staged,
+// each finished row divided by its power-of-two scale and the scale written to c_scale.
+template <class T, class TA, class ACC, int VB, int SG, bool FULL = false, bool SCALE = false>
 __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, unsigned sgmask,
                                           int2 *stage, ACC *vstage) {
+  static_assert(!SCALE || (sizeof(T) == 2 && sizeof(TA) == 4), "scaled walk: 16-bit B and C, FP32 values");
   // FP32 values ride in stage[].y; FP64 values are staged in vstage
   constexpr int UNR = 4;
   const int4 hdr = __ldg(reinterpret_cast<const int4 *>(a.task_hdr) + t);  // r, rn, hs, ts
@@ -316,6 +355,8 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
 #pragma unroll
         for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
       }
+    } else if constexpr (SCALE) {
+      store_scaled_row<T, ACC, VB, SG>(a, a.out_row ? __ldg(a.out_row + cur) : cur, sl, sgmask, acc, inb);
     } else if (inb) {
       const int orow = a.out_row ? __ldg(a.out_row + cur) : cur;
       vstore<T, ACC, VB>(static_cast<T *>(a.C) + (int64_t)orow * a.ldc + sl * VB, acc);
@@ -346,8 +387,14 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
       int2 e = make_int2(0, 0);
       if (j < m) {
         e.x = __ldcs(a.idx + q0 + j);
-        if constexpr (sizeof(TA) == 8) vstage[j] = (ACC)__ldcs(val + q0 + j);
-        else e.y = __float_as_int((float)__ldcs(val + q0 + j));
+        if constexpr (sizeof(TA) == 8) {
+          vstage[j] = (ACC)__ldcs(val + q0 + j);
+        } else if constexpr (SCALE) {  // B_true = b_scale * B (b_scale may be null)
+          const float bs = a.b_scale ? __ldg(a.b_scale + (e.x & 0x7fffffff)) : 1.f;
+          e.y = __float_as_int((float)__ldcs(val + q0 + j) * bs);
+        } else {
+          e.y = __float_as_int((float)__ldcs(val + q0 + j));
+        }
       }
       stage[j] = e;
     }
@@ -392,11 +439,11 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
 #pragma unroll
     for (int e = 0; e < VB; ++e) __stcg(dst + e, acc[e]);
   }
-  if (hdr.z >= 0 && hdr.x < hdr.y) arrive<T, ACC, VB, SG, 1>(a, hdr.z, sl, sgmask);
-  if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1>(a, hdr.w, sl, sgmask);
+  if (hdr.z >= 0 && hdr.x < hdr.y) arrive<T, ACC, VB, SG, 1, SCALE>(a, hdr.z, sl, sgmask);
+  if (hdr.w >= 0) arrive<T, ACC, VB, SG, 1, SCALE>(a, hdr.w, sl, sgmask);
 }
 
-template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL>
+template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL, bool SCALE = false>
 __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
   constexpr int G = 32 / SG;
   __shared__ int2 stage_all[8 * G][32];
@@ -406,7 +453,7 @@ __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a
   const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
   if (t >= a.ntasks) return;
   const int w = (threadIdx.x >> 5) * G + sg;
-  flag_walk<T, TA, ACC, VB, SG, FULL>(a, t, sl, sgmask, stage_all[w], vstage_all[sizeof(TA) == 8 ? w : 0]);
+  flag_walk<T, TA, ACC, VB, SG, FULL, SCALE>(a, t, sl, sgmask, stage_all[w], vstage_all[sizeof(TA) == 8 ? w : 0]);
 }
 
 // ---------------------------------------------------------------- staged walk
@@ -1039,13 +1086,13 @@ constexpr int flag_minb(int VB, int AB, int TB) {
   return b < 1 ? 1 : (b > 8 ? 8 : b);
 }
 
-template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL>
+template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL, bool SCALE = false>
 swift_status launch_flag(MergeArgs a, const int *eidx, cudaStream_t st) {
   constexpr int G = 32 / SG;
   const int64_t warps = ((int64_t)a.ntasks + G - 1) / G;
   if (warps == 0) return SWIFT_OK;
   a.idx = eidx;
-  merge_flag_kernel<T, TA, ACC, VB, SG, MINB, FULL><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
+  merge_flag_kernel<T, TA, ACC, VB, SG, MINB, FULL, SCALE><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(a);
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
 }
@@ -1082,6 +1129,25 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   constexpr int V = VecWidth<T>::value;
   constexpr int W = WideWidth<T>::value;
   constexpr int AB = (int)sizeof(ACC);
+  // per-row scales (16-bit B and C): the flagged walk with 16-byte vectors, one slice per lane
+  if (a.b_scale || a.c_scale) {
+    if constexpr (sizeof(T) == 2 && sizeof(TA) == 4) {
+      if (VB == V && VPL == 1 && a.N <= SG * V && a.c_scale && a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32)) {
+        constexpr int MB = flag_minb(V, AB, (int)sizeof(T));
+#define SW_SCALED(SG_)                                                                            \
+  if (SG == SG_)                                                                                  \
+    return a.N == SG_ * V ? launch_flag<T, TA, ACC, V, SG_, MB, true, true>(a, eidx, st)          \
+                          : launch_flag<T, TA, ACC, V, SG_, MB, false, true>(a, eidx, st);
+        SW_SCALED(2)
+        SW_SCALED(4)
+        SW_SCALED(8)
+        SW_SCALED(16)
+        SW_SCALED(32)
+#undef SW_SCALED
+      }
+    }
+    return SWIFT_ERR_UNSUPPORTED;
+  }
   // staged walk (kernel 4): FP32 values, B and C, one 16-byte slice per lane covering N;
   // unr selects the ring depth (16 slots = 3 groups of 4 rows in flight, or 32 = 7 groups)
   if constexpr (sizeof(T) == 4 && sizeof(TA) == 4 && sizeof(ACC) == 4) {
@@ -1189,6 +1255,8 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
   a.split_row = L.split_row.as<int>(); a.split_first = L.split_first.as<int>();
   a.split_last = L.split_last.as<int>(); a.split_cnt = L.split_cnt.as<int>();
   a.scratch = L.mscratch.p;
+  a.b_scale = d.b_scale;
+  a.c_scale = d.c_scale;
   const size_t esz = d.dtype == SWIFT_F64 ? 8 : (d.dtype == SWIFT_F32 ? 4 : 2);
   auto aligned = [&](int bytes) {
     return ((uintptr_t)d.B % bytes == 0) && ((uintptr_t)d.C % bytes == 0) &&
@@ -1198,7 +1266,9 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
   // vector width: 32 bytes when aligned and at most two vectors per lane cover the row slice,
   // else 16 bytes, else scalar
   int VB = 1;
-  if (o.vbytes != 16 && o.vbytes != 4 && aligned(32) && d.N / (int)(32 / esz) <= 64) VB = (int)(32 / esz);
+  const bool scaled = d.b_scale || d.c_scale;  // 16-byte vectors only (merge_shape checks the rest)
+  if (scaled && (esz != 2 || !aligned(16))) return SWIFT_ERR_UNSUPPORTED;
+  if (!scaled && o.vbytes != 16 && o.vbytes != 4 && aligned(32) && d.N / (int)(32 / esz) <= 64) VB = (int)(32 / esz);
   else if (o.vbytes != 4 && aligned(16)) VB = (int)(16 / esz);
   const int lanes = (d.N + VB - 1) / VB;
   int SG = 32, VPL = 1;

@@ -138,6 +138,7 @@ _SIGS = [
     ("swift_spmm_f64_reference", C.c_int, [_P, C.c_int, _P, _I64, _P, _I64, _P]),
     ("swift_plan_autotune", C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("swift_spmm_noalloc", C.c_int, [_P, C.c_int, C.c_int, _P, _I64, _P, _I64, _P]),
+    ("swift_spmm_scaled", C.c_int, [_P, C.c_int, C.c_int, _P, _I64, _P, _P, _I64, _P, _P]),
     ("swift_plan_set_rowwise_params", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("swift_plan_get_rowwise_params", C.c_int, [_P, C.c_int, C.c_int] + [C.POINTER(C.c_int)] * 4),
     ("swift_batch_create", C.c_int, [C.POINTER(_P), C.c_int, _P, C.POINTER(_P)]),

@@ -209,6 +209,27 @@ class Plan:
                                          _stream_ptr(stream)), "swift_spmm")
         return C_out
 
+    def spmm_scaled(self, B, b_scale=None, C_out=None, c_scale=None, stream=None):
+        """C, c_scale with A @ (b_scale[:, None] * B) == c_scale[:, None] * C: 16-bit (bf16 or
+        f16) row-major B and C scaled per row (swift_spmm_scaled).  b_scale: K floats or None
+        (all 1); c_scale is written with one power of two per row of C."""
+        torch = _torch()
+        N = int(B.shape[1])
+        if C_out is None:
+            C_out = torch.empty((self.M, N), dtype=B.dtype, device=B.device)
+        if c_scale is None:
+            c_scale = torch.empty(self.M, dtype=torch.float32, device=B.device)
+        if b_scale is not None and (b_scale.dtype != torch.float32 or b_scale.numel() != self.K
+                                    or not b_scale.is_contiguous()):
+            raise ValueError("b_scale must be a contiguous float32 tensor of K elements")
+        if c_scale.dtype != torch.float32 or c_scale.numel() != self.M or not c_scale.is_contiguous():
+            raise ValueError("c_scale must be a contiguous float32 tensor of M elements")
+        capi.check(capi.lib().swift_spmm_scaled(self._h, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, 0),
+                                                b_scale.data_ptr() if b_scale is not None else None,
+                                                C_out.data_ptr(), _ld(C_out, 0), c_scale.data_ptr(),
+                                                _stream_ptr(stream)), "swift_spmm_scaled")
+        return C_out, c_scale
+
     def spmm_t(self, Y, X_out=None, stream=None):
         """X = A^T @ Y (row-major)."""
         torch = _torch()

@@ -214,6 +214,72 @@ def test_low_precision_operands(dt16):
     pl.close()
 
 
+def _pow2_row_scale(x):
+    """Per-row powers of two putting each row's largest magnitude in [2^14, 2^15) (1 for zero rows)."""
+    m = np.abs(x).max(axis=1)
+    e = np.floor(np.log2(np.where(m > 0, m, 1.0)))
+    return np.where(m > 0, np.exp2(e - 14), 1.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("dt16", ["bf16", "f16"])
+@pytest.mark.parametrize("N", [8, 64, 128, 200, 256])
+@pytest.mark.parametrize("U", [32, 512])
+def test_per_row_scaled_16bit_operands(dt16, N, U):
+    """B rows spanning 2^-40 .. 2^40 (far outside FP16's range) stored as 16-bit rows with
+    per-row scales: every row of c_scale * C is within 1e-2 of the row's largest magnitude of
+    the FP64 product on the dequantised B, each c_scale is a power of two putting the row's
+    16-bit maximum in [2^14, 2^15], zero rows get scale 1, and rows split across tasks (U = 32)
+    combine deterministically."""
+    M, K, rp, ci = cases.make("rmat12", 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    rng = np.random.default_rng(7)
+    Btrue = gen.dense_uniform(K, N, 2, np.float64) * np.exp2(rng.integers(-40, 41, K))[:, None]
+    bs = _pow2_row_scale(Btrue)
+    tdt = torch.bfloat16 if dt16 == "bf16" else torch.float16
+    B16 = tdev((Btrue / bs[:, None]).astype(np.float32)).to(tdt)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    pl.set_rowwise_params(U, 4, 16, 2)
+    C16, cs = pl.spmm_scaled(B16, b_scale=tdev(bs))
+    C16b, csb = pl.spmm_scaled(B16, b_scale=tdev(bs))
+    assert torch.equal(C16, C16b) and torch.equal(cs, csb)
+    Bdeq = B16.double().cpu().numpy() * bs[:, None].astype(np.float64)
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, Bdeq)
+    C = C16.double().cpu().numpy()
+    s = cs.cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(C))
+    rmax = np.abs(ref).max(axis=1)
+    err = np.abs(s[:, None] * C - ref).max(axis=1)
+    assert np.all(err <= 1e-2 * rmax)
+    nz = rmax > 0
+    assert np.array_equal(np.exp2(np.round(np.log2(s))), s)  # powers of two
+    cmax = np.abs(C).max(axis=1)
+    assert np.all((cmax[nz] >= 2.0 ** 14) & (cmax[nz] <= 2.0 ** 15))
+    assert np.all(s[~nz] == 1.0) and np.all(C[~nz] == 0)
+    pl.close()
+
+
+def test_per_row_scaled_without_b_scale_and_refusals():
+    """b_scale omitted means all 1; F32 operands, widths above 256 and a missing c_scale are refused."""
+    M, K, rp, ci = cases.make("rmat12", 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    Bn = gen.dense_uniform(K, 64, 2, np.float32)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    B16 = tdev(Bn).to(torch.bfloat16)
+    C16, cs = pl.spmm_scaled(B16)
+    ref = oracle.csr_spmm_f64(M, K, rp, ci, val, B16.double().cpu().numpy())
+    got = cs.cpu().numpy()[:, None].astype(np.float64) * C16.double().cpu().numpy()
+    assert relerr(got, ref) <= 1e-2
+    from swift_b200 import _capi as capi
+    with pytest.raises(capi.SwiftError):
+        pl.spmm_scaled(tdev(Bn))
+    with pytest.raises(capi.SwiftError):
+        pl.spmm_scaled(tdev(gen.dense_uniform(K, 264, 2, np.float32)).to(torch.bfloat16))
+    st = capi.lib().swift_spmm_scaled(pl._h, 64, capi.BF16, B16.data_ptr(), 64, None, C16.data_ptr(), 64,
+                                      None, None)
+    assert st == capi.ERR_INVALID_ARG
+    pl.close()
+
+
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
 @pytest.mark.parametrize("name", ["rmat12", "skewed", "rect_wide", "rect_tall", "empty", "long_col"])
 def test_backward_products(name, dt):
