@@ -220,8 +220,8 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
  * term is A[r][k] * b_scale[k] * B[k][n], accumulated in F32.  C row r is written as
  * C_true[r] / c_scale[r] with c_scale[r] (M floats on the device) the power of two that
  * puts the row's largest magnitude in [2^14, 2^15) (1 for an all-zero row), so the 16-bit
- * rows neither overflow nor flush to zero.  Row walk only, N <= 256, B / C / ldb / ldc
- * 16-byte aligned; other shapes return SWIFT_ERR_UNSUPPORTED.  No counterpart in the
+ * rows neither overflow nor flush to zero.  Row walk only: B / C / ldb / ldc 16-byte aligned
+ * and N <= 256, or 32-byte aligned and N <= 512; other shapes return SWIFT_ERR_UNSUPPORTED.  No counterpart in the
  * reference (FP32 / FP64 only). */
 swift_status swift_spmm_scaled(const swift_plan *plan, int N, swift_dtype dtype, const void *B, int64_t ldb,
                                const float *b_scale, void *C, int64_t ldc, float *c_scale,

@@ -1129,20 +1129,26 @@ swift_status merge_shape(const MergeArgs &a, int VB, int SG, int VPL, int unr, i
   constexpr int V = VecWidth<T>::value;
   constexpr int W = WideWidth<T>::value;
   constexpr int AB = (int)sizeof(ACC);
-  // per-row scales (16-bit B and C): the flagged walk with 16-byte vectors, one slice per lane
+  // per-row scales (16-bit B and C): the flagged walk with 16- or 32-byte vectors, one slice
+  // per lane
   if (a.b_scale || a.c_scale) {
     if constexpr (sizeof(T) == 2 && sizeof(TA) == 4) {
-      if (VB == V && VPL == 1 && a.N <= SG * V && a.c_scale && a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32)) {
-        constexpr int MB = flag_minb(V, AB, (int)sizeof(T));
-#define SW_SCALED(SG_)                                                                            \
-  if (SG == SG_)                                                                                  \
-    return a.N == SG_ * V ? launch_flag<T, TA, ACC, V, SG_, MB, true, true>(a, eidx, st)          \
-                          : launch_flag<T, TA, ACC, V, SG_, MB, false, true>(a, eidx, st);
-        SW_SCALED(2)
-        SW_SCALED(4)
-        SW_SCALED(8)
-        SW_SCALED(16)
-        SW_SCALED(32)
+      if (VPL == 1 && a.N <= SG * VB && a.c_scale && a.ldb * (int64_t)sizeof(T) < (int64_t(1) << 32)) {
+#define SW_SCALED(VB_, SG_)                                                                              \
+  if (VB == VB_ && SG == SG_)                                                                            \
+    return a.N == SG_ * VB_                                                                              \
+               ? launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), true, true>(a, eidx, st) \
+               : launch_flag<T, TA, ACC, VB_, SG_, flag_minb(VB_, AB, (int)sizeof(T)), false, true>(a, eidx, st);
+        SW_SCALED(V, 2)
+        SW_SCALED(V, 4)
+        SW_SCALED(V, 8)
+        SW_SCALED(V, 16)
+        SW_SCALED(V, 32)
+        SW_SCALED(W, 2)
+        SW_SCALED(W, 4)
+        SW_SCALED(W, 8)
+        SW_SCALED(W, 16)
+        SW_SCALED(W, 32)
 #undef SW_SCALED
       }
     }
@@ -1266,10 +1272,11 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
   // vector width: 32 bytes when aligned and at most two vectors per lane cover the row slice,
   // else 16 bytes, else scalar
   int VB = 1;
-  const bool scaled = d.b_scale || d.c_scale;  // 16-byte vectors only (merge_shape checks the rest)
+  const bool scaled = d.b_scale || d.c_scale;  // 16- or 32-byte vectors (merge_shape checks the rest)
   if (scaled && (esz != 2 || !aligned(16))) return SWIFT_ERR_UNSUPPORTED;
-  if (!scaled && o.vbytes != 16 && o.vbytes != 4 && aligned(32) && d.N / (int)(32 / esz) <= 64) VB = (int)(32 / esz);
-  else if (o.vbytes != 4 && aligned(16)) VB = (int)(16 / esz);
+  if (o.vbytes != 16 && o.vbytes != 4 && aligned(32) && d.N / (int)(32 / esz) <= (scaled ? 32 : 64))
+    VB = (int)(32 / esz);
+  else if ((scaled || o.vbytes != 4) && aligned(16)) VB = (int)(16 / esz);
   const int lanes = (d.N + VB - 1) / VB;
   int SG = 32, VPL = 1;
   if (VB > 1) {

@@ -222,14 +222,16 @@ def _pow2_row_scale(x):
 
 
 @pytest.mark.parametrize("dt16", ["bf16", "f16"])
-@pytest.mark.parametrize("N", [8, 64, 128, 200, 256])
+@pytest.mark.parametrize("N", [8, 64, 96, 128, 200, 256, 512])
 @pytest.mark.parametrize("U", [32, 512])
-def test_per_row_scaled_16bit_operands(dt16, N, U):
+@pytest.mark.parametrize("vb", [0, 16])
+def test_per_row_scaled_16bit_operands(dt16, N, U, vb):
     """B rows spanning 2^-40 .. 2^40 (far outside FP16's range) stored as 16-bit rows with
     per-row scales: every row of c_scale * C is within 1e-2 of the row's largest magnitude of
     the FP64 product on the dequantised B, each c_scale is a power of two putting the row's
     16-bit maximum in [2^14, 2^15], zero rows get scale 1, and rows split across tasks (U = 32)
-    combine deterministically."""
+    combine deterministically.  vb = 0 lets rows of 16-element multiples take 32-byte vectors;
+    16 keeps 16-byte ones (up to N = 256)."""
     M, K, rp, ci = cases.make("rmat12", 0)
     val = gen.uniform_values(int(rp[-1]), 1, np.float32)
     rng = np.random.default_rng(7)
@@ -238,7 +240,13 @@ def test_per_row_scaled_16bit_operands(dt16, N, U):
     tdt = torch.bfloat16 if dt16 == "bf16" else torch.float16
     B16 = tdev((Btrue / bs[:, None]).astype(np.float32)).to(tdt)
     pl = Plan.from_csr(rp, ci, val, (M, K))
-    pl.set_rowwise_params(U, 4, 16, 2)
+    pl.set_rowwise_params(U, 4, vb, 2)
+    if vb == 16 and N > 256:
+        from swift_b200 import _capi as capi
+        with pytest.raises(capi.SwiftError):
+            pl.spmm_scaled(B16, b_scale=tdev(bs))
+        pl.close()
+        return
     C16, cs = pl.spmm_scaled(B16, b_scale=tdev(bs))
     C16b, csb = pl.spmm_scaled(B16, b_scale=tdev(bs))
     assert torch.equal(C16, C16b) and torch.equal(cs, csb)
