@@ -35,6 +35,31 @@ def _stream_ptr(stream=None):
     return C.c_void_p(s.cuda_stream)
 
 
+def _dense(t, rows, cols, name, dtype=None):
+    """Checks an operand before its pointer reaches a kernel: a 2-D CUDA tensor of rows x cols
+    (and dtype); a wrong shape or a host tensor would otherwise be read or written out of bounds."""
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or t.dim() != 2:
+        raise ValueError(f"{name} must be a 2-D tensor")
+    if tuple(t.shape) != (rows, cols):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected ({rows}, {cols})")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name} has dtype {t.dtype}, expected {dtype}")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    return t
+
+
+def _vec(t, n, name, dtype):
+    """As _dense for a contiguous 1-D CUDA tensor of n elements of dtype."""
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or t.numel() != n or not t.is_contiguous() or t.dtype != dtype:
+        raise ValueError(f"{name} must be a contiguous {dtype} tensor of {n} elements")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    return t
+
+
 def _ld(t, layout):
     if t.dim() != 2:
         raise ValueError("dense operands are 2-D")
@@ -199,10 +224,12 @@ class Plan:
         torch = _torch()
         lay = capi.ROW_MAJOR if layout == "row" else capi.COL_MAJOR
         N = int(B.shape[1])
+        _dense(B, self.K, N, "B")
         if C_out is None:
             C_out = torch.empty((self.M, N), dtype=B.dtype, device=B.device)
             if lay == capi.COL_MAJOR:
                 C_out = torch.empty((N, self.M), dtype=B.dtype, device=B.device).t()
+        _dense(C_out, self.M, N, "C_out", B.dtype)
         eng = {"auto": capi.ENGINE_AUTO, "tiled": capi.ENGINE_TILED, "rowwise": capi.ENGINE_ROWWISE}[engine]
         capi.check(capi.lib().swift_spmm(self._h, eng, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, lay), lay,
                                          int(b_presorted), C_out.data_ptr(), _ld(C_out, lay), lay,
@@ -215,15 +242,15 @@ class Plan:
         (all 1); c_scale is written with one power of two per row of C."""
         torch = _torch()
         N = int(B.shape[1])
+        _dense(B, self.K, N, "B")
         if C_out is None:
             C_out = torch.empty((self.M, N), dtype=B.dtype, device=B.device)
+        _dense(C_out, self.M, N, "C_out", B.dtype)
         if c_scale is None:
             c_scale = torch.empty(self.M, dtype=torch.float32, device=B.device)
-        if b_scale is not None and (b_scale.dtype != torch.float32 or b_scale.numel() != self.K
-                                    or not b_scale.is_contiguous()):
-            raise ValueError("b_scale must be a contiguous float32 tensor of K elements")
-        if c_scale.dtype != torch.float32 or c_scale.numel() != self.M or not c_scale.is_contiguous():
-            raise ValueError("c_scale must be a contiguous float32 tensor of M elements")
+        if b_scale is not None:
+            _vec(b_scale, self.K, "b_scale", torch.float32)
+        _vec(c_scale, self.M, "c_scale", torch.float32)
         capi.check(capi.lib().swift_spmm_scaled(self._h, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, 0),
                                                 b_scale.data_ptr() if b_scale is not None else None,
                                                 C_out.data_ptr(), _ld(C_out, 0), c_scale.data_ptr(),
@@ -234,8 +261,10 @@ class Plan:
         """X = A^T @ Y (row-major)."""
         torch = _torch()
         N = int(Y.shape[1])
+        _dense(Y, self.M, N, "Y")
         if X_out is None:
             X_out = torch.empty((self.K, N), dtype=Y.dtype, device=Y.device)
+        _dense(X_out, self.K, N, "X_out", Y.dtype)
         capi.check(capi.lib().swift_spmm_transposed(self._h, N, _dtype_code(Y.dtype), Y.data_ptr(),
                                                     _ld(Y, 0), X_out.data_ptr(), _ld(X_out, 0),
                                                     _stream_ptr(stream)), "swift_spmm_transposed")
@@ -245,9 +274,12 @@ class Plan:
         """out[e] = U[row_e] . V[col_e] for every nonzero e in CSR order."""
         torch = _torch()
         N = int(U.shape[1])
+        _dense(U, self.M, N, "U")
+        _dense(V, self.K, N, "V", U.dtype)
         vt = torch.float64 if self.val_dtype == np.float64 else torch.float32
         if out is None:
             out = torch.empty(self.nnz, dtype=vt, device=U.device)
+        _vec(out, self.nnz, "out", vt)
         capi.check(capi.lib().swift_sddmm(self._h, N, _dtype_code(U.dtype), U.data_ptr(), _ld(U, 0),
                                           V.data_ptr(), _ld(V, 0), out.data_ptr(), _stream_ptr(stream)),
                    "swift_sddmm")
@@ -262,6 +294,14 @@ class Plan:
             dX = torch.empty((self.K, N), dtype=X.dtype, device=X.device)
         if "dA" in want and dA is None:
             dA = torch.empty(self.nnz, dtype=X.dtype, device=X.device)
+        _dense(X, self.K, N, "X")
+        _dense(dY, self.M, N, "dY", X.dtype)
+        if Y is not None:
+            _dense(Y, self.M, N, "Y", X.dtype)
+        if dX is not None:
+            _dense(dX, self.K, N, "dX", X.dtype)
+        if dA is not None:
+            _vec(dA, self.nnz, "dA", X.dtype)
 
         def p(t):
             return t.data_ptr() if t is not None else None
@@ -276,6 +316,7 @@ class Plan:
     def spmm_f64_reference(self, B64, stream=None):
         torch = _torch()
         N = int(B64.shape[1])
+        _dense(B64, self.K, N, "B64", torch.float64)
         out = torch.empty((self.M, N), dtype=torch.float64, device=B64.device)
         capi.check(capi.lib().swift_spmm_f64_reference(self._h, N, B64.data_ptr(), _ld(B64, 0),
                                                        out.data_ptr(), _ld(out, 0), _stream_ptr(stream)),
@@ -301,6 +342,8 @@ class Plan:
         ms = C.c_double(0)
         eng = C.c_int(0)
         N = int(B.shape[1])
+        _dense(B, self.K, N, "B")
+        _dense(C_out, self.M, N, "C_out", B.dtype)
         capi.check(capi.lib().swift_plan_autotune(self._h, N, _dtype_code(B.dtype), B.data_ptr(),
                                                   C_out.data_ptr(), _stream_ptr(stream), C.byref(ms),
                                                   C.byref(eng)), "swift_plan_autotune")
@@ -328,6 +371,10 @@ class Batch:
         n = len(self.plans)
         if len(Bs) != n or len(Cs) != n:
             raise ValueError("one B and one C per plan")
+        torch = _torch()
+        for i, (p, b, c) in enumerate(zip(self.plans, Bs, Cs)):
+            _dense(b, p.K, int(b.shape[1]) if b.dim() == 2 else -1, f"Bs[{i}]", torch.float32)
+            _dense(c, p.M, int(b.shape[1]), f"Cs[{i}]", torch.float32)
         Ns = (C.c_int * max(n, 1))(*[int(b.shape[1]) for b in Bs])
         Bp = (C.c_void_p * max(n, 1))(*[b.data_ptr() for b in Bs])
         Cp = (C.c_void_p * max(n, 1))(*[c.data_ptr() for c in Cs])

@@ -340,3 +340,28 @@ def test_bad_csr_rejected():
     ci = np.array([0, 1, 9], np.int32)
     with pytest.raises(capi.SwiftError):
         Plan.from_csr(tdev(rp), tdev(ci), tdev(np.ones(3, np.float32)), (3, 3))
+
+
+def test_python_layer_refuses_bad_operands_before_launch():
+    """Wrong shapes, dtypes and host tensors are refused on the host by every product method."""
+    M, K, rp, ci = cases.make("rmat12", 0)
+    val = gen.uniform_values(int(rp[-1]), 1, np.float32)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    B = tdev(gen.dense_uniform(K, 32, 2, np.float32))
+    with pytest.raises(ValueError, match="shape"):
+        pl.spmm(B[:-1])
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        pl.spmm(B.cpu())
+    with pytest.raises(ValueError, match="dtype"):
+        pl.spmm(B, C_out=torch.empty((M, 32), dtype=torch.float64, device="cuda"))
+    with pytest.raises(ValueError, match="shape"):
+        pl.spmm_t(B[:, :16].contiguous()[: M - 1])
+    with pytest.raises(ValueError, match="shape"):
+        pl.sddmm(B, B[:-1])
+    with pytest.raises(ValueError, match="elements"):
+        pl.spmm_scaled(B.to(torch.bfloat16), b_scale=torch.ones(K - 1, device="cuda"))
+    with pytest.raises(ValueError, match="shape"):
+        pl.autotune(B, torch.empty((M, 16), device="cuda"))
+    C = pl.spmm(B)  # still usable
+    assert relerr(C.cpu().numpy(), oracle.csr_spmm_f64(M, K, rp, ci, val, B.cpu().numpy())) <= 1e-5
+    pl.close()
