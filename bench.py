@@ -12,7 +12,8 @@ Several GPUs run independent replicas (the product has no exchange step).
 
 --impl reference times the reference's own CPU product (Swift_cpu, compiled from the
 reference sources under oracle/_ref; the oracle's restatement if that build is absent) on
-the host cores: each step is a bounded sample of tiles of the same workload.
+the host cores: each step is one whole product of the same workload (or, where warm-up and
+steps would not fit --ref-seconds, the next equal share of one, in the reference's order).
 
 --mtx FILE [--n N] [--dtype f32|f64] runs the same product on a MatrixMarket file (the
 reference's input format) instead of a synthetic matrix.
@@ -217,17 +218,38 @@ def profile_summary(workload):
 
 class _StdoutToStderr:
     """Routes C-level stdout to stderr (the reference's host code prints progress and
-    diagnostic lines; stdout carries only the JSON line)."""
+    diagnostic lines; stdout carries only the JSON line).
+
+    One line is known to be spurious and is labelled as such on its way through: the
+    reference's csr2csc prints "CSR 2 CSC error" whenever the last CSR value differs from
+    the last CSC value (src/coo2csc.h:57-63), which is the normal case for any matrix whose
+    last row and last column end in different nonzeros.  Every other line passes unchanged,
+    so a real failure message still reads as one."""
+    KNOWN = {"CSR 2 CSC error": "the reference's last-value comparison (src/coo2csc.h:57-63), "
+                                "not a failure: its CSC is correct and is checked bit for bit"}
 
     def __enter__(self):
+        import tempfile
         sys.stdout.flush()
         self.saved = os.dup(1)
-        os.dup2(2, 1)
+        self.tmp = tempfile.TemporaryFile(mode="w+b")
+        os.dup2(self.tmp.fileno(), 1)
 
     def __exit__(self, *exc):
+        import ctypes
+        try:
+            ctypes.CDLL(None).fflush(None)  # C stdio buffers of the reference code
+        except Exception:
+            pass
         sys.stdout.flush()
         os.dup2(self.saved, 1)
         os.close(self.saved)
+        self.tmp.seek(0)
+        for raw in self.tmp.read().decode(errors="replace").splitlines():
+            note = self.KNOWN.get(raw.strip())
+            sys.stderr.write(f"{raw}   [{note}]\n" if note else raw + "\n")
+        sys.stderr.flush()
+        self.tmp.close()
 
 
 def cpu_swift(M, K, rp, ci, val_np, B_np, N, impl="ref"):
@@ -256,23 +278,59 @@ def _cpu_swift(M, K, rp, ci, val_np, B_np, N, impl):
     return cs, use
 
 
-def run_cpu_samples(cs, seconds, warm=1):
-    """Time consecutive tile ranges until `seconds` of CPU work; returns (GFLOP/s, sample)."""
-    T = cs.tilenum
-    chunk = max(1, min(T, 4096))
-    t = 0
-    for _ in range(warm):
-        cs.run(0, min(chunk, T))
-    tot_s, tot_nnz, ranges = 0.0, 0, 0
-    while tot_s < seconds and T > 0:
-        t1 = min(T, t + chunk)
-        s, n = cs.run(t, t1)
+def cpu_product(cs):
+    """One whole Swift_cpu product (every regular tile and the reside part) into a zeroed C,
+    as the reference's driver calls it on a freshly allocated result (src/main.cu:302).
+    Returns (seconds, nonzeros)."""
+    cs.C.fill(0)
+    return cs.run(0, cs.tilenum, with_reside=True)
+
+
+def run_cpu_products(cs, seconds):
+    """Whole products repeated within `seconds` of CPU time (at least one; an untimed one
+    first when three fit).  Returns (GFLOP/s, seconds timed, nonzeros, products timed)."""
+    s0, n = cpu_product(cs)
+    tot_s, prods = 0.0, 0
+    if 3 * s0 > seconds:  # too slow for a warm-up: the first product is the sample
+        tot_s, prods = s0, 1
+    while prods == 0 or tot_s + tot_s / prods <= seconds:
+        s, n = cpu_product(cs)
         tot_s += s
-        tot_nnz += n
-        ranges += 1
-        t = 0 if t1 >= T else t1
-    gf = 2.0 * tot_nnz * cs.N / tot_s / 1e9 if tot_s > 0 else 0.0
-    return gf, tot_s, tot_nnz
+        prods += 1
+    gf = 2.0 * n * prods * cs.N / tot_s / 1e9 if tot_s > 0 else 0.0
+    return gf, tot_s, n * prods, prods
+
+
+def oracle_call(name, *a):
+    """One call of an oracle restatement (test-side C code, used here only as the CPU baseline)."""
+    import oracle
+    return getattr(oracle, name)(*a)
+
+
+def cpu_port_line(fn, flops, seconds, what):
+    """CPU baseline from an oracle restatement where the reference has no implementation: fn
+    repeated within `seconds` (at least once), flops per call."""
+    try:
+        n, tot = 0, 0.0
+        while n == 0 or tot + tot / n <= seconds:
+            a = time.perf_counter()
+            fn()
+            tot += time.perf_counter() - a
+            n += 1
+        return {"value": flops * n / tot / 1e9, "unit": "GFLOP/s", "cores": 1, "kind": "port",
+                "sample": f"{what}: {n} whole call(s) in {tot:.1f} s, one thread"}
+    except Exception as ex:  # the baseline is reported, never required
+        return {"value": None, "unit": "GFLOP/s", "cores": 1, "kind": "port", "sample": f"failed: {ex}"}
+
+
+def cpu_baseline_line(cs, kind, seconds, what):
+    gf, secs, snnz, prods = run_cpu_products(cs, seconds)
+    return {"value": gf, "unit": "GFLOP/s", "cores": 1,
+            "kind": "reference" if kind == "ref" else "port",
+            "host_preprocessing_ms": getattr(cs, "preprocessing_ms", None),
+            "sample": f"{what}: {prods} whole Swift_cpu product(s) of this workload ({snnz // max(prods, 1)} nonzeros "
+                      f"x N={cs.N} each) in {secs:.1f} s; single-threaded by construction, as the reference is "
+                      f"(host has {os.cpu_count()} threads)"}
 
 
 # ------------------------------------------------------------------------------------ ours
@@ -307,6 +365,54 @@ def _timed(fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
+def _gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    return vis.split(",")[local] if vis else local
+
+
+def _timed_clocked(fn, steps, warmup, local=0):
+    """As _timed, with nvidia-smi clocks and throttle reasons sampled over the timed region:
+    returns (device ms per call, clocks record)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(_gpu_index(local))
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop(w0, time.time())
+    return e0.elapsed_time(e1) / steps, clocks
+
+
+def merge_clocks(recs):
+    """One clocks record over several timed regions: median of their medians, every reason."""
+    recs = [r for r in recs if r]
+    if not recs:
+        return None
+    return {"sm_mhz": statistics.median(r["sm_mhz"] for r in recs), "sm_max_mhz": recs[0]["sm_max_mhz"],
+            "reasons": sorted(set().union(*[set(r["reasons"]) for r in recs])),
+            "samples": sum(r["samples"] for r in recs), "regions": len(recs)}
+
+
+def roofline_line(alg_bytes, ms, workload, default_kernel):
+    """The roofline record of the line's dominant kernel: algorithmic bytes / device time
+    against the measured copy bandwidth, and the DRAM traffic of the committed ncu summary."""
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    prof = profile_summary(workload)
+    traffic = float(prof["dram_bytes_per_launch"].split()[0]) if prof else None
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "traffic_source": prof.get("file"), "kernel": prof.get("kernel", default_kernel),
+            "peak_source": f"{peak_kind} ({'MEASURED_PEAKS.json hbm_gbs' if peak_kind == 'measured' else 'pool fallback'})",
+            "algorithmic_bytes_per_launch": alg_bytes}
+
+
 def _single_gpu_line(args, out):
     rank = int(os.environ.get("RANK", "0"))
     if rank == 0:
@@ -330,11 +436,12 @@ def run_precision(args):
     ref = plan.spmm_f64_reference(B32.double())
     refmax = ref.abs().max().item()
     res = {}
+    peak = hbm_peak()[0]
     for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
         B = B32.to(dt)
         C = torch.empty((M, N), dtype=dt, device="cuda")
         eng, _ = plan.autotune(B, C)
-        ms = _timed(lambda: plan.spmm(B, C), args.steps, args.warmup)
+        ms, clk = _timed_clocked(lambda: plan.spmm(B, C), args.steps, args.warmup, local)
         plan.spmm(B, C)
         err = (C.double() - ref).abs().max().item() / refmax
         # error of the 16-bit result against the same product on 16-bit-rounded inputs in FP64
@@ -342,10 +449,11 @@ def run_precision(args):
         if dt != torch.float32:
             ref_q = plan.spmm_f64_reference(B.double())
             err_in = (C.double() - ref_q).abs().max().item() / ref_q.abs().max().item()
+            del ref_q
         bytes_ = nnz * 8 + (K + M) * N * B.element_size()
         res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": eng,
                      "err_vs_fp64": err, "err_vs_fp64_on_rounded_B": err_in,
-                     "algorithmic_bytes": bytes_, "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / hbm_peak()[0]}
+                     "algorithmic_bytes": bytes_, "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / peak, "clocks": clk}
     # 16-bit B and C with per-row power-of-two scales (swift_spmm_scaled): B rows stored as
     # B / b_scale with each row's maximum in [2^14, 2^15); error of c_scale * C against FP64
     m = B32.abs().amax(dim=1)
@@ -355,24 +463,41 @@ def run_precision(args):
         B = (B32 / bscale[:, None]).to(dt)
         C = torch.empty((M, N), dtype=dt, device="cuda")
         cs = torch.empty(M, dtype=torch.float32, device="cuda")
-        ms = _timed(lambda: plan.spmm_scaled(B, b_scale=bscale, C_out=C, c_scale=cs), args.steps, args.warmup)
+        ms, clk = _timed_clocked(lambda: plan.spmm_scaled(B, b_scale=bscale, C_out=C, c_scale=cs), args.steps,
+                                 args.warmup, local)
         plan.spmm_scaled(B, b_scale=bscale, C_out=C, c_scale=cs)
         err = (C.double() * cs.double()[:, None] - ref).abs().max().item() / refmax
         bytes_ = nnz * 8 + (K + M) * (N * B.element_size() + 4)
         res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": "rowwise",
                      "err_vs_fp64": err, "algorithmic_bytes": bytes_,
-                     "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / hbm_peak()[0]}
+                     "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / peak, "clocks": clk}
+    del ref
     f32b, bfb = res["f32"]["algorithmic_bytes"], res["bf16"]["algorithmic_bytes"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:  # the reference has no 16-bit path: its FP32 Swift_cpu on the same matrix and B
+            cs_, kind = cpu_swift(M, K, rp, ci, val.cpu().numpy(), B32.cpu().numpy(), N, impl="ref")
+            cpu = cpu_baseline_line(cs_, kind, args.cpu_seconds,
+                                    "the reference's FP32 Swift_cpu (it has no BF16/FP16 path)")
+            del cs_
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
     out = {
         "metric": "spmm_gflops", "value": res["bf16"]["gflops"], "unit": "GFLOP/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["bf16"]["ms"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 B/C, fp32 accumulate", "data": "synthetic",
         "config": {"workload": args.workload, "rows": M, "nnz_realised": nnz, "N": N,
+                   "l2": "inputs larger than L2 (B and C exceed 126 MB in every precision); no flush between steps",
                    "description": describe(args.workload, dict(wl, kind="rmatband", dtype="bf16/f16/f32"), nnz)},
         "ratio_bf16_vs_f32": res["f32"]["ms"] / res["bf16"]["ms"],
         "ratio_f16_vs_f32": res["f32"]["ms"] / res["f16"]["ms"],
         "byte_model_ceiling_16bit_vs_f32": f32b / bfb,
+        "roofline": roofline_line(bfb, res["bf16"]["ms"], args.workload, "merge_flag_kernel"),
         "products": res,
+        "gpu_launches": args.steps,
+        "clocks": merge_clocks([r["clocks"] for r in res.values()]),
+        "clocks_headline": res["bf16"]["clocks"],
+        "cpu_baseline": cpu,
     }
     _single_gpu_line(args, out)
 
@@ -396,13 +521,10 @@ def run_sddmm(args):
     V = torch.rand((K, N), generator=g, device="cuda") * 2 - 1
     plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
     out = torch.empty(nnz, device="cuda")
-    ms = _timed(lambda: plan.sddmm(U, V, out), args.steps, args.warmup)
+    Un, Vn = (None, None) if args.no_cpu_baseline else (U.double().cpu().numpy(), V.double().cpu().numpy())
+    ms, clocks = _timed_clocked(lambda: plan.sddmm(U, V, out), args.steps, args.warmup, local)
     flops = 2.0 * nnz * N
     alg_bytes = nnz * (4 + 4) + M * N * 4 + K * N * 4
-    peak, peak_kind = hbm_peak()
-    achieved = alg_bytes / (ms / 1e3) / 1e9
-    prof = profile_summary(args.workload)
-    traffic = float(prof["dram_bytes_per_launch"].split()[0]) if prof else None
     library = None
     try:
         A_t = torch.sparse_csr_tensor(torch.from_numpy(rp).cuda().long(), torch.from_numpy(ci).cuda().long(),
@@ -423,10 +545,12 @@ def run_sddmm(args):
         "config": {"workload": args.workload, "description": describe(args.workload, wl, nnz), "rows": M,
                    "cols": K, "nnz": nnz, "N": N,
                    "l2": "inputs larger than L2 (U and V exceed 126 MB); no flush between steps"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "traffic_source": prof.get("file"), "kernel": prof.get("kernel", "merge_bwd_kernel"),
-                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg_bytes},
+        "roofline": roofline_line(alg_bytes, ms, args.workload, "merge_bwd_kernel"),
         "gpu_launches": args.steps,
+        "clocks": clocks,
+        "cpu_baseline": None if args.no_cpu_baseline else cpu_port_line(
+            lambda: oracle_call("sddmm_f64", M, K, rp, ci, Un, Vn), flops, args.cpu_seconds,
+            "the oracle's FP64 SDDMM restatement (the reference has no SDDMM)"),
         "library_context": library,
     }
     _single_gpu_line(args, res)
@@ -467,16 +591,30 @@ def run_fwdbwd(args):
     def fused():
         plan.fused_forward_backward(X, dY, Y, dX, dA)
 
-    t_plain = _timed(plain, args.steps, args.warmup)
+    clk = {}
+    t_plain, clk["plain"] = _timed_clocked(plain, args.steps, args.warmup, local)
     symmetric = plan.is_symmetric()
     plan.set_symmetry(False)  # general path: Y and dA in one pass, dX over A^T
-    t_fused_general = _timed(fused, args.steps, args.warmup)
+    t_fused_general, clk["fused_general"] = _timed_clocked(fused, args.steps, args.warmup, local)
     plan.set_symmetry(True)
-    t_fused = _timed(fused, args.steps, args.warmup)
-    t_fwd = _timed(lambda: plan.spmm(X, Y), args.steps, args.warmup)
-    t_bwd = _timed(lambda: plan.spmm_t(dY, dX), args.steps, args.warmup)
-    t_sddmm = _timed(lambda: plan.sddmm(dY, X, dA), args.steps, args.warmup)
+    t_fused, clk["fused"] = _timed_clocked(fused, args.steps, args.warmup, local)
+    t_fwd, clk["spmm"] = _timed_clocked(lambda: plan.spmm(X, Y), args.steps, args.warmup, local)
+    t_bwd, clk["spmm_t"] = _timed_clocked(lambda: plan.spmm_t(dY, dX), args.steps, args.warmup, local)
+    t_sddmm, clk["sddmm"] = _timed_clocked(lambda: plan.sddmm(dY, X, dA), args.steps, args.warmup, local)
     flops = 3 * 2.0 * nnz * N
+    # fused pass over symmetric A: A once (value + index), X and dY read once, Y, dX and dA written once
+    alg_bytes = nnz * (8 + 4) + 4 * M * N * 4
+    cpu = None
+    if not args.no_cpu_baseline:
+        Xn, dYn = X.double().cpu().numpy(), dY.double().cpu().numpy()
+        v64 = vals.astype(np.float64)
+
+        def port():
+            oracle_call("csr_spmm_f64", M, M, rp, ci, v64, Xn)
+            oracle_call("csr_spmm_t_f64", M, M, rp, ci, v64, dYn)
+            oracle_call("sddmm_f64", M, M, rp, ci, dYn, Xn)
+        cpu = cpu_port_line(port, flops, args.cpu_seconds, "the oracle's FP64 restatements of Y = A X, "
+                            "dX = A^T dY and dA = SDDMM(dY, X) (the reference has no backward pass)")
     out = {
         "metric": "spmm_gflops", "value": flops / (t_fused / 1e3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fused, "higher_is_better": True,
@@ -491,6 +629,11 @@ def run_fwdbwd(args):
         "paths": {"plain": "swift_spmm + swift_spmm_transposed + swift_sddmm, each its own pass",
                   "fused": "one pass over A for Y, dX (A symmetric: dX = A dY) and dA",
                   "fused_general": "one pass over A for Y and dA, one over A^T for dX"},
+        "roofline": roofline_line(alg_bytes, t_fused, args.workload, "merge_bwd_kernel"),
+        "gpu_launches": args.steps,
+        "clocks": merge_clocks(list(clk.values())),
+        "clocks_by_region": clk,
+        "cpu_baseline": cpu,
     }
     _single_gpu_line(args, out)
 
@@ -538,7 +681,11 @@ def run_batch(args):
         rows_tot += M
     batch = Batch(plans)
     batch.set_operands(Bs, Cs)
+    torch.cuda.synchronize()
+    tw0 = time.perf_counter()
     best_U, tune_ms = batch.autotune()
+    torch.cuda.synchronize()
+    tune_wall_ms = (time.perf_counter() - tw0) * 1e3
     for _ in range(args.warmup):
         batch.run_graph()
     stream = torch.cuda.current_stream()
@@ -631,7 +778,8 @@ def run_batch(args):
                 "average degree U[4, 64], half uniform-random and half R-MAT; N from {32, 64, 128})",
         "config": {"workload": args.workload, "matrices": len(mats), "rows": rows_tot, "nnz": nnz_tot,
                    "N_counts": {str(n): Ns.count(n) for n in (32, 64, 128)}, "task_size": best_U,
-                   "autotune_ms": tune_ms, "launch": "one persistent kernel per step, replayed as a CUDA graph",
+                   "autotune_wall_ms": tune_wall_ms, "autotune_best_candidate_ms": tune_ms,
+                   "launch": "one persistent kernel per step, replayed as a CUDA graph",
                    "l2": "B and C of the batch (about 5 GB) exceed L2; no flush between steps",
                    "parallelism": f"replicas x{world} (no exchange step)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -684,9 +832,13 @@ def run_ours(args):
     if args.rowwise_params:
         U, unr, vb, kern = (int(x) for x in args.rowwise_params.split(","))
         plan.set_rowwise_params(U, unr, vb, kern)
-        engine, tune_ms = "rowwise", 0.0
+        engine, tune_ms, tune_wall_ms = "rowwise", None, 0.0
     else:
+        torch.cuda.synchronize()
+        tw0 = time.perf_counter()
         engine, tune_ms = plan.autotune(B, C)
+        torch.cuda.synchronize()
+        tune_wall_ms = (time.perf_counter() - tw0) * 1e3
     rw_params = plan.rowwise_params(N, B.dtype) if engine == "rowwise" else None
     st = plan.stats()
     stream = torch.cuda.current_stream()
@@ -822,12 +974,7 @@ def run_ours(args):
             cs, kind = cpu_swift(M, K, rp, ci, val.cpu().numpy(),
                                  B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy(),
                                  N, impl="ref")
-            gf, secs, snnz = run_cpu_samples(cs, args.cpu_seconds)
-            cpu = {"value": gf, "unit": "GFLOP/s", "cores": 1,
-                   "kind": "reference" if kind == "ref" else "port",
-                   "host_preprocessing_ms": cs.preprocessing_ms,
-                   "sample": f"Swift_cpu over consecutive tile ranges of this workload: {snnz} nonzeros x N={N} "
-                             f"in {secs:.1f} s (single-threaded by construction; host has {os.cpu_count()} threads)"}
+            cpu = cpu_baseline_line(cs, kind, args.cpu_seconds, "the reference's Swift_cpu (oracle/_ref)")
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GFLOP/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
 
@@ -847,7 +994,8 @@ def run_ours(args):
                    "row_engine_params": rw_params,
                    "parallelism": f"replicas x{world} (no exchange step)",
                    "l2": "inputs larger than L2 (B and C exceed 126 MB); no flush between steps",
-                   "plan_build_ms": st["build_ms"], "autotune_ms": tune_ms,
+                   "plan_build_ms": st["build_ms"], "autotune_wall_ms": tune_wall_ms,
+                   "autotune_best_candidate_ms": tune_ms,
                    "format": {k: st[k] for k in ("nsteps", "tilenum", "reside_col", "reside_nnz", "numblk",
                                                   "fmt_count", "long_rows", "long_pieces", "max_row_nnz")}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -888,37 +1036,58 @@ def run_reference(args):
         dev = "cpu"
     if wl["kind"] == "batch":
         return run_reference_batch(args, wl, dev)
-    if wl["kind"] in ("sddmm", "fwdbwd", "precision"):
+    if wl["kind"] in ("sddmm", "fwdbwd"):
         print(json.dumps({"impl": "reference", "unavailable": f"the reference has no CPU path for the "
                           f"{wl['kind']} workload (SpMM only)"}), flush=True)
         return
+    note = None
+    if wl["kind"] == "precision":
+        # the reference has no 16-bit operands: its FP32 Swift_cpu on the same matrix and B
+        wl = dict(wl, kind=wl["rk"], dtype="f32")
+        note = "the reference has no BF16/FP16 path; this is its FP32 Swift_cpu on the same matrix and B"
     M, K, rp, ci, val, B = make_inputs(wl, dev)
     import torch
     Bn = B.float().cpu().numpy() if B.dtype in (torch.bfloat16, torch.float16) else B.cpu().numpy()
     vn = val.cpu().numpy()
     nnz = int(rp[-1])
     cs, kind = cpu_swift(M, K, rp, ci, vn, Bn, N, impl="ref")
+    del Bn
     T = cs.tilenum
-    # size each step so that warmup + steps take about a minute of CPU time
-    s, n = cs.run(0, min(T, 256))
-    per_tile = s / max(1, min(T, 256))
-    budget = float(args.ref_seconds)
-    chunk = int(max(1, min(T, budget / max(1, args.steps + args.warmup) / max(per_tile, 1e-9))))
-    t = 0
+    # a step is one whole product when warm-up + steps fit the time budget; otherwise each
+    # step is the next of S equal shares of the tiles (the reside part with the last share),
+    # so that S consecutive steps make one whole product in the reference's own order
+    t_prod, _ = cpu_product(cs)
+    S = 1
+    while S < max(T, 1) and (args.steps + args.warmup) * t_prod / S > float(args.ref_seconds):
+        S *= 2
+    j = 0
+
+    def step():
+        nonlocal j
+        if j == 0:
+            cs.C.fill(0)
+        t0, t1 = j * T // S, (j + 1) * T // S
+        r = cs.run(t0, t1, with_reside=(j == S - 1))
+        j = (j + 1) % S
+        return r
+
     for _ in range(args.warmup):
-        t1 = min(T, t + chunk)
-        cs.run(t, t1)
-        t = 0 if t1 >= T else t1
+        step()
     tot_s, tot_nnz = 0.0, 0
     for _ in range(args.steps):
-        t1 = min(T, t + chunk)
-        sec, n = cs.run(t, t1)
+        sec, n = step()
         tot_s += sec
         tot_nnz += n
-        t = 0 if t1 >= T else t1
     value = 2.0 * tot_nnz * N / tot_s / 1e9 if tot_s > 0 else 0.0
-    sample = (f"each step: Swift_cpu over {chunk} consecutive tiles ({chunk * 32} nonzeros x N={N}) of this workload; "
-              f"{tot_nnz} nonzeros in {tot_s:.2f} s over {args.steps} steps")
+    if S == 1:
+        sample = (f"each step: one whole Swift_cpu product of this workload ({nnz} nonzeros x N={N}) into a zeroed C; "
+                  f"{args.steps} products in {tot_s:.2f} s")
+    else:
+        sample = (f"each step: the next 1/{S} of the tiles of one whole Swift_cpu product in the reference's order "
+                  f"({S} steps make a product of {nnz} nonzeros x N={N}; a whole product takes {t_prod:.2f} s); "
+                  f"{tot_nnz} nonzeros in {tot_s:.2f} s over {args.steps} steps")
+    if note:
+        sample += f"; {note}"
     out = {
         "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": tot_s * 1e3 / max(1, args.steps), "higher_is_better": True,
@@ -1003,7 +1172,7 @@ def run_reference_gpu(args):
     plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
     C = torch.empty((M, N), dtype=B.dtype, device="cuda")
     engine, _ = plan.autotune(B, C)
-    lib_ms = _timed(lambda: plan.spmm(B, C), max(5, min(args.steps, 200)), args.warmup)
+    lib_ms, lib_clocks = _timed_clocked(lambda: plan.spmm(B, C), max(5, min(args.steps, 200)), args.warmup)
     plan.spmm(B, C)
     golden = C.cpu().numpy()
     plan.close()
@@ -1021,6 +1190,9 @@ def run_reference_gpu(args):
     fmt4 = dict(fmt, sortrowidx=sl.arrays["rowsorted_rowidx"])
     reps = max(1, min(args.steps, 5))
     variants = {}
+    sampler = ClockSampler(_gpu_index(0))
+    sampler.start()
+    w0 = time.time()
     for var, name in oracle.REF_GPU_VARIANTS.items():
         f = fmt4 if var == 4 else fmt
         if not oracle.ref_gpu_accepts(var, f, N, sB.dtype):
@@ -1043,6 +1215,7 @@ def run_reference_gpu(args):
         diff = float(np.abs(np.asarray(Cr, np.float64) - golden).max() / max(np.abs(golden).max(), 1e-300))
         variants[name] = {"status": "ok (reference check passed)", "ms": ms, "gflops": flops / (ms / 1e3) / 1e9,
                           "max_rel_diff_vs_library": diff}
+    ref_clocks = sampler.stop(w0, time.time())
     ok = [x for x in variants.values() if "ms" in x]
     best = min(ok, key=lambda x: x["ms"]) if ok else None
     out = {
@@ -1057,7 +1230,9 @@ def run_reference_gpu(args):
                   "check outside; median of the calls after the first",
         "variants": variants,
         "library": {"engine": engine, "ms": lib_ms, "gflops": flops / (lib_ms / 1e3) / 1e9,
-                    "speedup_vs_best_reference_kernel": (best["ms"] / lib_ms) if best else None},
+                    "speedup_vs_best_reference_kernel": (best["ms"] / lib_ms) if best else None,
+                    "clocks": lib_clocks},
+        "clocks": ref_clocks,
     }
     print(json.dumps(out), flush=True)
 
@@ -1071,7 +1246,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--ref-seconds", type=float, default=60.0)
+    ap.add_argument("--ref-seconds", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rowwise-params", help="task_size,loads_in_flight,vector_bytes,kernel: run the row "
                                              "engine with these instead of autotuning (e.g. for a profile)")

@@ -277,7 +277,11 @@ swift_status swift_spmm_f64_reference(const swift_plan *plan, int N, const doubl
  * of partial rows within the array minus 64 KiB; larger products return SWIFT_ERR_OVERFLOW
  * (details in swift_last_error) -- a plan made with a larger long_row_split has fewer pieces.
  * The first call on each device looks up the array's device address with that device
- * current, so make it before any stream capture.  All calls share the array and it keeps the
+ * current, so make it before any stream capture.  The address is kept per device together
+ * with the id of the CUDA context it belongs to; if that context is destroyed and a new one
+ * made (cudaDeviceReset), the next call looks the address up again in the new context -- make
+ * that call, too, outside stream capture, after creating new plans (a reset also destroys every
+ * plan's device memory).  All calls share the array and it keeps the
  * last call's contents (each call clears the counters it uses): calls that overlap on the GPU
  * race, so serialise them. */
 #define SWIFT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)

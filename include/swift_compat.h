@@ -330,6 +330,41 @@ inline int mmio_allinone(int *m, int *n, int *nnz, int *isSymmetric, int **csrro
   return swift_compat_detail::mmio(m, n, nnz, isSymmetric, csrrowptr, csrcolidx, csrval, filename, SWIFT_F32);
 }
 
+/* ---------------------------------------------------------------- driver-level macros
+ * What the reference's drivers take from its headers besides functions: the tile size
+ * (src/auxiliary.h:6-8), the file the drivers append their result line to (src/auxiliary.h:22;
+ * test/k-32/FP32/auxiliary.h:22 for the FP32 flavour), and the two error checks that the
+ * reference's cuSPARSE harness (src/gpu_cusparse_spmm.h) expands, defined in its
+ * src/gpu_csr2csc.h:4-22: report the failed call with its line and carry on. */
+#ifndef TILESIZE
+#define TILESIZE 32
+#endif
+#ifndef RESULT_FILE_PATH
+#ifdef SWIFT_COMPAT_FP32
+#define RESULT_FILE_PATH "./data/results_Swift_FP32_32.txt"
+#else
+#define RESULT_FILE_PATH "./data/results_Swift_32.txt"
+#endif
+#endif
+#ifndef CHECK_CUDA
+#define CHECK_CUDA(call)                                                                         \
+  {                                                                                              \
+    const cudaError_t swift_compat_rc_ = (call);                                                 \
+    if (swift_compat_rc_ != cudaSuccess)                                                         \
+      std::printf("swift_compat: CUDA call at line %d failed: %s (%d)\n", __LINE__,               \
+                  cudaGetErrorString(swift_compat_rc_), (int)swift_compat_rc_);                   \
+  }
+#endif
+#ifndef CHECK_CUSPARSE
+#define CHECK_CUSPARSE(call)                                                                     \
+  {                                                                                              \
+    const cusparseStatus_t swift_compat_sp_ = (call);                                            \
+    if (swift_compat_sp_ != CUSPARSE_STATUS_SUCCESS)                                             \
+      std::printf("swift_compat: cuSPARSE call at line %d failed: %s (%d)\n", __LINE__,           \
+                  cusparseGetErrorString(swift_compat_sp_), (int)swift_compat_sp_);               \
+  }
+#endif
+
 /* ---------------------------------------------------------------- src/format.h:48 */
 inline void Tile_destroy(swift_slide_matrix_f64 *matrix) { swift_slide_free_f64(matrix); }
 inline void Tile_destroy(swift_slide_matrix_f32 *matrix) { swift_slide_free_f32(matrix); }

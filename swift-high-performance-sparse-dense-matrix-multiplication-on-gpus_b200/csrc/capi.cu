@@ -189,10 +189,45 @@ swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
   return SWIFT_OK;
 }
 
+namespace swift {
+void note_use(Plan &p, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  std::lock_guard<std::mutex> g(p.use_mu);
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    p.sync_device_on_destroy = true;  // replayed later, on whatever stream the graph runs on
+    return;
+  }
+  for (auto &u : p.uses)
+    if (u.first == st) {
+      cudaEventRecord(u.second, st);
+      return;
+    }
+  cudaEvent_t ev = nullptr;
+  if ((int)p.uses.size() >= Plan::kMaxUses ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    p.sync_device_on_destroy = true;
+    return;
+  }
+  cudaEventRecord(ev, st);
+  p.uses.emplace_back(st, ev);
+}
+
+UseNote::~UseNote() { note_use(p, st); }
+
+Plan::~Plan() {
+  // the device buffers are freed after this body: wait for the work that reads them
+  if (sync_device_on_destroy) {
+    cudaDeviceSynchronize();
+  } else {
+    for (auto &u : uses) cudaEventSynchronize(u.second);
+  }
+  for (auto &u : uses) cudaEventDestroy(u.second);
+}
+}  // namespace swift
+
 swift_status swift_plan_destroy(swift_plan *plan) {
   if (!plan) return SWIFT_ERR_INVALID_ARG;
-  cudaDeviceSynchronize();
-  delete plan;
+  delete plan;  // ~Plan waits for the plan's own streams (every stream if graphs hold it)
   return SWIFT_OK;
 }
 
@@ -218,6 +253,7 @@ swift_status swift_plan_set_values(swift_plan *plan, const void *val, swift_mems
   if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
   if (p.nnz > 0 && !val) return SWIFT_ERR_INVALID_ARG;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  UseNote use_note{p, st};
   std::lock_guard<std::mutex> g(p.mu);
   if (p.nnz > 0)
     SW_CHECK_CUDA(cudaMemcpyAsync(p.val.p, val, p.vsz * (size_t)p.nnz,
@@ -292,6 +328,7 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
   d.N = N; d.dtype = dtype; d.B = B; d.ldb = ldb; d.b_layout = b_layout; d.b_presorted = b_presorted != 0;
   d.C = C; d.ldc = ldc; d.c_layout = c_layout;
   cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
   const bool row_ok = p.has_csr && b_layout == SWIFT_ROW_MAJOR && c_layout == SWIFT_ROW_MAJOR && !b_presorted;
   // Column-major operands: in that layout each nonzero's N contributions land M elements apart,
   // so the row walk runs on row-major copies instead (B transposed in, C transposed out through
@@ -355,6 +392,7 @@ swift_status swift_spmm_scaled(const swift_plan *plan, int N, swift_dtype dtype,
   d.N = N; d.dtype = dtype; d.B = B; d.ldb = ldb; d.C = C; d.ldc = ldc;
   d.b_scale = b_scale;
   d.c_scale = c_scale;
+  UseNote use_note{p, S(stream)};
   return run_merge(p, p.fwd, d, merge_opts_for(p, N, dtype), S(stream));
 }
 
@@ -366,6 +404,7 @@ swift_status swift_spmm_transposed(const swift_plan *plan, int N, swift_dtype dt
   Plan &p = const_cast<Plan &>(plan->p);
   if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
   SW_TRY(ensure_bwd(p, st));
   if (p.K == 0 || N == 0) return SWIFT_OK;
   DenseArgs d;
@@ -383,6 +422,7 @@ swift_status swift_sddmm(const swift_plan *plan, int N, swift_dtype dtype, const
   if (p.nnz > 0 && !out) return SWIFT_ERR_INVALID_ARG;
   if (p.nnz == 0) return SWIFT_OK;
   cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
   if (N == 0) {
     SW_CHECK_CUDA(cudaMemsetAsync(out, 0, p.vsz * (size_t)p.nnz, st));
     return SWIFT_OK;
@@ -401,6 +441,7 @@ swift_status swift_plan_set_symmetry(swift_plan *plan, int use) {
 
 swift_status swift_plan_is_symmetric(swift_plan *plan, int *symmetric, swift_stream_t stream) {
   if (!plan || !symmetric) return SWIFT_ERR_INVALID_ARG;
+  UseNote use_note{plan->p, S(stream)};
   SW_TRY(check_symmetric(plan->p, S(stream)));
   *symmetric = plan->p.symmetric;
   return SWIFT_OK;
@@ -416,6 +457,7 @@ swift_status swift_fused_forward_backward(const swift_plan *plan, int N, swift_d
   if (dtype != SWIFT_F32 && dtype != SWIFT_F64) return SWIFT_ERR_UNSUPPORTED;
   SW_TRY(check_dense(plan, N, dtype, X, ldx, SWIFT_ROW_MAJOR, p.K, dY, lddy, SWIFT_ROW_MAJOR, p.M));
   cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
   if (N == 0) return SWIFT_OK;
   if (Y && dA && dX && p.use_symmetry) {
     // A == A^T with equal values: dX = A dY joins the same pass over A
@@ -449,6 +491,7 @@ swift_status swift_spmm_f64_reference(const swift_plan *plan, int N, const doubl
                                       int64_t ldb, double *C, int64_t ldc,
                                       swift_stream_t stream) {
   if (!plan || N < 0 || (N > 0 && (!B || !C)) || ldb < N || ldc < N) return SWIFT_ERR_INVALID_ARG;
+  UseNote use_note{const_cast<Plan &>(plan->p), S(stream)};
   return run_f64_reference(plan->p, N, B, ldb, C, ldc, S(stream));
 }
 
@@ -458,6 +501,7 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
   if (!plan || !B || !C || N <= 0) return SWIFT_ERR_INVALID_ARG;
   Plan &p = plan->p;
   cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

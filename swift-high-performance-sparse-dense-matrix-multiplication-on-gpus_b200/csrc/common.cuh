@@ -198,6 +198,23 @@ struct Plan {
   // row-major copies of column-major dense operands for the row walk (grown on demand)
   DevBuf rowcopy_b, rowcopy_c;
   std::mutex mu;  // guards lazily built layouts and scratch growth
+  // Streams this plan's work was enqueued on, each with an event recorded after its latest
+  // call, so that destroying the plan waits for its own work only.  Work captured into a CUDA
+  // graph (and streams beyond kMaxUses) can run later on any stream: then destruction waits
+  // for the whole device.
+  static constexpr int kMaxUses = 16;
+  std::mutex use_mu;
+  std::vector<std::pair<cudaStream_t, cudaEvent_t>> uses;
+  bool sync_device_on_destroy = false;
+  ~Plan();
+};
+
+// Records that `st` holds work on this plan; UseNote does it when an entry point returns.
+void note_use(Plan &p, cudaStream_t st);
+struct UseNote {
+  Plan &p;
+  cudaStream_t st;
+  ~UseNote();
 };
 
 size_t plan_device_bytes(const Plan &p);

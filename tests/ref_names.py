@@ -1,4 +1,5 @@
-"""The reference's preprocessing and SpMM functions under their own names (host numpy buffers).
+"""Test helper: the reference's preprocessing and SpMM functions under their own names (host
+numpy buffers), so that the compatibility tests read like the reference's driver.
 
 Each function calls the matching ``swift_ref_*`` entry point of libswiftb200.so, which runs the
 stage on the GPU.  Names, argument meanings and the order of calls follow the reference driver
@@ -27,7 +28,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import _capi as capi
+from swift_b200 import _capi as capi
 
 _libc = C.CDLL(None)
 _libc.free.argtypes = [C.c_void_p]
@@ -225,7 +226,7 @@ def mmio_allinone(filename, dtype=np.float64):
 
     rc is the reference's return code (0, -1 cannot open, -2 banner, -4 size line) or -5 where
     the reference would go on with undefined values; the arrays are None unless rc == 0."""
-    from .mtx import read_mtx, reference_code
+    from swift_b200.mtx import read_mtx, reference_code
     try:
         mm = read_mtx(filename, dtype)
     except capi.SwiftError:

@@ -12,7 +12,8 @@ import pytest
 
 import golden_io
 import oracle
-from swift_b200 import capi, compat
+import ref_names as compat
+from swift_b200 import capi
 
 pytestmark = pytest.mark.gpu
 

@@ -16,7 +16,7 @@ import pytest
 
 import oracle
 from swift_b200 import capi
-from swift_b200 import compat
+import ref_names as compat
 from swift_b200.mtx import read_mtx, reference_code
 
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
