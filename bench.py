@@ -707,8 +707,6 @@ def run_batch(args):
     ms = max_over_ranks(ms, dist)
     ms_step = ms / args.steps
     value = whole_job_rate(flops * args.steps, world, ms / 1e3) / 1e9
-    peak, peak_kind = hbm_peak()
-    achieved = alg_bytes / (ms_step / 1e3) / 1e9
     # end to end: every member's B in from pinned host memory, every C out.  Copies in, the
     # batch and copies out run on three streams over two operand sets (a second batch object
     # over the same plans), so one step's C leaves while the next step's B arrives.
@@ -769,6 +767,15 @@ def run_batch(args):
         dist.destroy_process_group()
     if rank != 0:
         return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            gf, secs, done, kind = cpu_batch_products(mats, args.cpu_seconds)
+            cpu = {"value": gf, "unit": "GFLOP/s", "cores": 1, "kind": "reference" if kind == "ref" else "port",
+                   "sample": f"the reference's Swift_cpu over whole products of the first {done} of {len(mats)} "
+                             f"members in {secs:.1f} s (single-threaded by construction, as the reference is)"}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GFLOP/s", "cores": 1, "kind": "reference", "sample": f"failed: {ex}"}
     Ns = [m["N"] for m in mats]
     out = {
         "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world,
@@ -782,16 +789,14 @@ def run_batch(args):
                    "launch": "one persistent kernel per step, replayed as a CUDA graph",
                    "l2": "B and C of the batch (about 5 GB) exceed L2; no flush between steps",
                    "parallelism": f"replicas x{world} (no exchange step)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": peak_kind, "kernel": "merge_batch_kernel",
-                     "algorithmic_bytes_per_launch": alg_bytes},
+        "roofline": roofline_line(alg_bytes, ms_step, args.workload, "merge_batch_kernel"),
         "e2e": {"value": world * flops * n_e2e / (e2e_ms / 1e3) / 1e9, "unit": "GFLOP/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": n_e2e,
                 "ms_per_step": e2e_ms / n_e2e,
                 "pipeline": "one H2D / the batch / one D2H per step on three streams, two operand sets"},
         "gpu_launches": args.steps,
         "clocks": clocks,
-        "cpu_baseline": None,
+        "cpu_baseline": cpu,
     }
     print(json.dumps(out), flush=True)
     batch.close()
@@ -1103,12 +1108,9 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def run_reference_batch(args, wl, dev):
-    """The reference's Swift_cpu over the batch members in order (whole products), until the
-    time budget is spent; value = flops of the products run / their time."""
-    from swift_b200 import gen
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    mats = gen.batch_matrices(wl["count"], seed=0, device=dev)
+def cpu_batch_products(mats, seconds):
+    """The reference's Swift_cpu over the batch members in order (whole products, each into a
+    zeroed C), until `seconds` of CPU time; returns (GFLOP/s, seconds, members done, kind)."""
     rng = np.random.default_rng(1)
     tot_s = tot_f = 0.0
     done = 0
@@ -1119,13 +1121,22 @@ def run_reference_batch(args, wl, dev):
         val = rng.uniform(-1, 1, nnz).astype(np.float32)
         B = rng.uniform(-1, 1, (M, N)).astype(np.float32)
         cs, kind = cpu_swift(M, M, m["rowptr"], m["colidx"], val, B, N, impl="ref")
-        sec, n = cs.run(0, cs.tilenum, with_reside=True)
+        sec, n = cpu_product(cs)
         tot_s += sec
         tot_f += 2.0 * n * N
         done += 1
-        if tot_s >= args.ref_seconds:
+        if tot_s >= seconds:
             break
-    value = tot_f / tot_s / 1e9 if tot_s > 0 else 0.0
+    return (tot_f / tot_s / 1e9 if tot_s > 0 else 0.0), tot_s, done, kind
+
+
+def run_reference_batch(args, wl, dev):
+    """The reference's Swift_cpu over the batch members in order (whole products), until the
+    time budget is spent; value = flops of the products run / their time."""
+    from swift_b200 import gen
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    mats = gen.batch_matrices(wl["count"], seed=0, device=dev)
+    value, tot_s, done, kind = cpu_batch_products(mats, args.ref_seconds)
     sample = f"Swift_cpu over whole products of the first {done} of {len(mats)} matrices in {tot_s:.2f} s"
     out = {
         "metric": "spmm_gflops", "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": done,

@@ -82,9 +82,19 @@ typedef enum swift_memspace { SWIFT_HOST = 0, SWIFT_DEVICE = 1 } swift_memspace;
  *              in registers and written once; rows longer than the split threshold are cut
  *              into pieces combined deterministically.  Column-major B or C are transposed
  *              into row-major copies held by the plan (not with b_presorted).
+ *   TILED_GROUPED -- the tiled engine in the order of Swift_GPU_4 (src/Swift_4.h:6-76): the
+ *              slots of every group of 8 tiles visited in row-sorted order (the per-group row
+ *              sort of src/back_process.h:23-229, run on the GPU when first needed), so equal
+ *              rows of a group form one run and take one vector atomic.  Row-major B and C,
+ *              FP32 or FP64.
  *   AUTO    -- the autotuned choice for (N, dtype), ROWWISE when no tuning was run and the
  *              layouts allow it. */
-typedef enum swift_engine { SWIFT_ENGINE_AUTO = 0, SWIFT_ENGINE_TILED = 1, SWIFT_ENGINE_ROWWISE = 2 } swift_engine;
+typedef enum swift_engine {
+  SWIFT_ENGINE_AUTO = 0,
+  SWIFT_ENGINE_TILED = 1,
+  SWIFT_ENGINE_ROWWISE = 2,
+  SWIFT_ENGINE_TILED_GROUPED = 3
+} swift_engine;
 
 typedef struct swift_csr {
   int rows;              /* M */

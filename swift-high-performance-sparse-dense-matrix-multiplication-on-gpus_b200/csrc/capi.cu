@@ -97,6 +97,42 @@ swift_status ensure_bwd(Plan &p, cudaStream_t st) {
 
 using namespace swift;
 
+namespace swift {
+void note_use(Plan &p, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  std::lock_guard<std::mutex> g(p.use_mu);
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    p.sync_device_on_destroy = true;  // replayed later, on whatever stream the graph runs on
+    return;
+  }
+  for (auto &u : p.uses)
+    if (u.first == st) {
+      cudaEventRecord(u.second, st);
+      return;
+    }
+  cudaEvent_t ev = nullptr;
+  if ((int)p.uses.size() >= Plan::kMaxUses ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    p.sync_device_on_destroy = true;
+    return;
+  }
+  cudaEventRecord(ev, st);
+  p.uses.emplace_back(st, ev);
+}
+
+UseNote::~UseNote() { note_use(p, st); }
+
+Plan::~Plan() {
+  // the device buffers are freed after this body: wait for the work that reads them
+  if (sync_device_on_destroy) {
+    cudaDeviceSynchronize();
+  } else {
+    for (auto &u : uses) cudaEventSynchronize(u.second);
+  }
+  for (auto &u : uses) cudaEventDestroy(u.second);
+}
+}  // namespace swift
+
 extern "C" {
 
 const char *swift_status_string(swift_status s) {
@@ -189,41 +225,6 @@ swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
   return SWIFT_OK;
 }
 
-namespace swift {
-void note_use(Plan &p, cudaStream_t st) {
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  std::lock_guard<std::mutex> g(p.use_mu);
-  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
-    p.sync_device_on_destroy = true;  // replayed later, on whatever stream the graph runs on
-    return;
-  }
-  for (auto &u : p.uses)
-    if (u.first == st) {
-      cudaEventRecord(u.second, st);
-      return;
-    }
-  cudaEvent_t ev = nullptr;
-  if ((int)p.uses.size() >= Plan::kMaxUses ||
-      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
-    p.sync_device_on_destroy = true;
-    return;
-  }
-  cudaEventRecord(ev, st);
-  p.uses.emplace_back(st, ev);
-}
-
-UseNote::~UseNote() { note_use(p, st); }
-
-Plan::~Plan() {
-  // the device buffers are freed after this body: wait for the work that reads them
-  if (sync_device_on_destroy) {
-    cudaDeviceSynchronize();
-  } else {
-    for (auto &u : uses) cudaEventSynchronize(u.second);
-  }
-  for (auto &u : uses) cudaEventDestroy(u.second);
-}
-}  // namespace swift
 
 swift_status swift_plan_destroy(swift_plan *plan) {
   if (!plan) return SWIFT_ERR_INVALID_ARG;
@@ -255,6 +256,7 @@ swift_status swift_plan_set_values(swift_plan *plan, const void *val, swift_mems
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   UseNote use_note{p, st};
   std::lock_guard<std::mutex> g(p.mu);
+  p.grouped_built = false;  // rebuilt from the new slot values on its next use
   if (p.nnz > 0)
     SW_CHECK_CUDA(cudaMemcpyAsync(p.val.p, val, p.vsz * (size_t)p.nnz,
                                   mem == SWIFT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
@@ -375,6 +377,15 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
     return run_merge(p, p.fwd, d, merge_opts_for(p, N, dtype), st);
   }
   if (engine == SWIFT_ENGINE_TILED) return run_tiled(p, d, 0, st);
+  if (engine == SWIFT_ENGINE_TILED_GROUPED) {
+    if (b_layout != SWIFT_ROW_MAJOR || c_layout != SWIFT_ROW_MAJOR) return SWIFT_ERR_UNSUPPORTED;
+    if (dtype == SWIFT_BF16 || dtype == SWIFT_F16) return SWIFT_ERR_UNSUPPORTED;
+    {
+      std::lock_guard<std::mutex> g(p.mu);
+      if (!p.grouped_built) SW_TRY(build_grouped(p, nullptr, nullptr, st));
+    }
+    return run_tiled(p, d, 0, st, true);
+  }
   return SWIFT_ERR_INVALID_ARG;
 }
 
@@ -510,7 +521,10 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
     MergeOpts mo;
   };
   std::vector<Cand> cands;
-  if (dtype != SWIFT_BF16 && dtype != SWIFT_F16) cands.push_back({SWIFT_ENGINE_TILED, MergeOpts{}});
+  if (dtype != SWIFT_BF16 && dtype != SWIFT_F16) {
+    cands.push_back({SWIFT_ENGINE_TILED, MergeOpts{}});
+    cands.push_back({SWIFT_ENGINE_TILED_GROUPED, MergeOpts{}});
+  }
   if (p.has_csr) {
     // task size (the work-balance grain) x (loads in flight, vector bytes, kernel variant)
     const int shapes[][3] = {{4, 16, 1}, {8, 16, 1}, {4, 32, 1}, {4, 16, 2}, {4, 32, 2}};

@@ -197,6 +197,10 @@ struct Plan {
   int use_symmetry = 1;
   // row-major copies of column-major dense operands for the row walk (grown on demand)
   DevBuf rowcopy_b, rowcopy_c;
+  // grouped tiled engine: the regular slots of every 8-tile group in row-sorted order -- C row,
+  // sorted column and value per sorted slot (built on first use; new values invalidate it)
+  DevBuf g_row, g_col, g_val;
+  bool grouped_built = false;
   std::mutex mu;  // guards lazily built layouts and scratch growth
   // Streams this plan's work was enqueued on, each with an event recorded after its latest
   // call, so that destroying the plan waits for its own work only.  Work captured into a CUDA
@@ -280,7 +284,13 @@ struct DenseArgs {
   float *c_scale = nullptr;
 };
 // variant 1 = reside per column without balance blocks (Swift_gpu1's kernel)
-swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cudaStream_t st);
+swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cudaStream_t st,
+                       bool grouped = false);
+// The grouped engine's slots (p.g_row, p.g_col, p.g_val) from the regular tiles.  keys and
+// vpos: the per-group sorted rows and each original slot's sorted position, as row_idx_sort
+// leaves them (src/back_process.h:23-229); both null to sort p.sortrowidx here.  A vpos that is
+// not a permutation of each group returns SWIFT_ERR_INVALID_ARG.
+swift_status build_grouped(Plan &p, const int *keys, const int *vpos, cudaStream_t st);
 swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &a, cudaStream_t st);
 swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpts &o,
                        cudaStream_t st);

@@ -53,26 +53,6 @@ __global__ void dense_row_gather_kernel(const int *__restrict__ perm, const T *_
   }
 }
 
-// After row_idx_sort the slot keys are sorted within each group of 8 tiles (256 slots) and
-// val_position[j] is where slot j's key went (src/back_process.h:52-80); Swift_GPU_4 pairs
-// sortval[j] with sortrowidx[group + val_position[j]] (src/Swift_4.h:30-47).  This restores
-// the unsorted key of every slot; a position outside its group sets *bad.
-__global__ void unsort_rows_kernel(const int *__restrict__ sorted, const int *__restrict__ vpos,
-                                   int64_t nreg, int *__restrict__ out, int *__restrict__ bad) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nreg; j += stride) {
-    const int64_t g = j & ~(int64_t)255;
-    const int64_t glen = nreg - g < 256 ? nreg - g : 256;
-    const int v = vpos[j];
-    if (v < 0 || v >= glen) {
-      *bad = 1;
-      out[j] = 0;
-    } else {
-      out[j] = sorted[g + v];
-    }
-  }
-}
-
 int grid_warps(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n * 32 + 255) / 256, 148 * 32));
 }
@@ -402,23 +382,18 @@ swift_status ref_spmm(int variant, const SLIDE *m, int rowA, int colA, int width
   SW_TRY(upload(p.tile_colidx, m->tile_colidx, (size_t)m->tilenum, st));
   SW_TRY(upload(p.sortrowidx, m->sortrowidx, nreg, st));
   SW_TRY(upload(p.sortval, m->sortval, nreg, st));
-  if (variant == 4 && m->val_position && nreg > 0) {
-    DevBuf vpos, keys, bad;
+  // Swift_GPU_4 runs after row_idx_sort: sortrowidx holds each group's sorted rows and
+  // val_position maps every original slot to its sorted one (src/back_process.h:23-229); the
+  // grouped engine walks exactly that order
+  const bool grouped = variant == 4 && m->val_position && nreg > 0;
+  if (grouped) {
+    DevBuf vpos;
     SW_TRY(upload(vpos, m->val_position, nreg, st));
-    SW_TRY(keys.alloc(sizeof(int) * nreg));
-    SW_TRY(bad.alloc(sizeof(int)));
-    SW_CHECK_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
-    unsort_rows_kernel<<<grid_warps((int64_t)(nreg + 31) / 32), 256, 0, st>>>(
-        p.sortrowidx.as<int>(), vpos.as<int>(), (int64_t)nreg, keys.as<int>(), bad.as<int>());
-    SW_CHECK_LAUNCH();
-    int hbad = 0;
-    SW_CHECK_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SW_CHECK_CUDA(cudaStreamSynchronize(st));
-    if (hbad) {
-      set_last_error("Swift_GPU_4", "val_position outside its group of 8 tiles");
-      return SWIFT_ERR_INVALID_ARG;
+    const swift_status rc = build_grouped(p, p.sortrowidx.as<int>(), vpos.as<int>(), st);
+    if (rc != SWIFT_OK) {
+      set_last_error("Swift_GPU_4", "val_position is not a permutation of each group of 8 tiles");
+      return rc;
     }
-    p.sortrowidx = std::move(keys);
   }
   p.reside_col = m->reside_col;
   p.reside_nnz = m->reside_nnz;
@@ -452,7 +427,7 @@ swift_status ref_spmm(int variant, const SLIDE *m, int rowA, int colA, int width
   d.ldb = d.ldc = std::max(width, 1);
   Timer tm(st);
   if (colmajor) SW_TRY(transpose_dense(B.p, colA, width, colA, Bt.p, width, sizeof(T), st));
-  SW_TRY(run_tiled(p, d, variant == 1 ? 1 : 0, st));
+  SW_TRY(run_tiled(p, d, variant == 1 ? 1 : 0, st, grouped));
   if (colmajor) SW_TRY(transpose_dense(Ct.p, width, rowA, width, C.p, rowA, sizeof(T), st));
   const float t = tm.stop();
   if (ms) *ms = t;

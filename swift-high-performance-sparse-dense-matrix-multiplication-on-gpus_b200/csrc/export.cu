@@ -94,6 +94,26 @@ __global__ void row_sort_kernel(const int *__restrict__ rows, int T, int *__rest
   if (i == 0 && !non_single) atomicAdd(all_single_groups, 1);
 }
 
+// Grouped-engine slots: original slot o of group g lands at sorted slot g*256 + vpos[o], with
+// its sorted column (tile_colidx of its tile + lane) and value; a vpos entry outside its group
+// or hit twice sets *bad (with n slots per group and no slot hit twice, every slot is filled).
+template <class V>
+__global__ void grouped_scatter_kernel(const int *__restrict__ vpos, const int *__restrict__ tile_colidx,
+                                       const V *__restrict__ sortval, int64_t nreg, int *__restrict__ col,
+                                       V *__restrict__ val, int *__restrict__ hit, int *__restrict__ bad) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nreg; o += stride) {
+    const int64_t g = o & ~(int64_t)255;
+    const int64_t glen = nreg - g < 256 ? nreg - g : 256;
+    const int v = vpos[o];
+    if (v < 0 || v >= glen) { *bad = 1; continue; }
+    const int64_t s = g + v;
+    if (atomicExch(hit + s, 1) != 0) { *bad = 1; continue; }
+    col[s] = tile_colidx[o >> 5] + (int)(o & 31);
+    val[s] = sortval[o];
+  }
+}
+
 int grid_warps(int64_t warps) {
   int64_t b = (warps * 32 + 255) / 256;
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
@@ -110,6 +130,54 @@ template <class T> T *host_copy(const void *dev, size_t n, cudaStream_t st, swif
 }
 
 }  // namespace
+
+swift_status build_grouped(Plan &p, const int *keys, const int *vpos, cudaStream_t st) {
+  const int T = p.tilenum;
+  const int64_t nreg = (int64_t)T * kTile;
+  if ((keys == nullptr) != (vpos == nullptr)) return SWIFT_ERR_INVALID_ARG;
+  p.grouped_built = false;
+  SW_TRY(p.g_row.alloc(sizeof(int) * (size_t)std::max<int64_t>(nreg, 1)));
+  SW_TRY(p.g_col.alloc(sizeof(int) * (size_t)std::max<int64_t>(nreg, 1)));
+  SW_TRY(p.g_val.alloc(p.vsz * (size_t)std::max<int64_t>(nreg, 1)));
+  if (nreg == 0) {
+    p.grouped_built = true;
+    return SWIFT_OK;
+  }
+  TmpBuf tvpos, toff, hit, flags;
+  SW_TRY(hit.alloc(sizeof(int) * (size_t)nreg, st));
+  SW_TRY(flags.alloc(sizeof(int) * 2, st));
+  SW_CHECK_CUDA(cudaMemsetAsync(hit.p, 0, sizeof(int) * (size_t)nreg, st));
+  SW_CHECK_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * 2, st));
+  if (!keys) {
+    SW_TRY(tvpos.alloc(sizeof(int) * (size_t)nreg, st));
+    SW_TRY(toff.alloc(sizeof(int) * (size_t)nreg, st));
+    row_sort_kernel<<<(T + 7) / 8, 256, 0, st>>>(p.sortrowidx.as<int>(), T, p.g_row.as<int>(), tvpos.as<int>(),
+                                                  toff.as<int>(), flags.as<int>() + 1);
+    SW_CHECK_LAUNCH();
+    vpos = tvpos.as<int>();
+  } else {
+    SW_CHECK_CUDA(cudaMemcpyAsync(p.g_row.p, keys, sizeof(int) * (size_t)nreg, cudaMemcpyDeviceToDevice, st));
+  }
+  const int grid = grid_warps((nreg + 31) / 32);
+  if (p.val_type == SWIFT_F64)
+    grouped_scatter_kernel<double><<<grid, 256, 0, st>>>(vpos, p.tile_colidx.as<int>(), p.sortval.as<double>(), nreg,
+                                                         p.g_col.as<int>(), p.g_val.as<double>(), hit.as<int>(),
+                                                         flags.as<int>());
+  else
+    grouped_scatter_kernel<float><<<grid, 256, 0, st>>>(vpos, p.tile_colidx.as<int>(), p.sortval.as<float>(), nreg,
+                                                        p.g_col.as<int>(), p.g_val.as<float>(), hit.as<int>(),
+                                                        flags.as<int>());
+  SW_CHECK_LAUNCH();
+  int bad = 0;
+  SW_CHECK_CUDA(cudaMemcpyAsync(&bad, flags.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (bad) {
+    set_last_error("grouped slots", "val_position is not a permutation of each group of 8 tiles");
+    return SWIFT_ERR_INVALID_ARG;
+  }
+  p.grouped_built = true;
+  return SWIFT_OK;
+}
 
 swift_status build_segments(const Plan &p, DevBuf &countrow, DevBuf &segmentoffset,
                             DevBuf &sortrowindex, int *segsum, cudaStream_t st) {

@@ -38,6 +38,10 @@ struct TiledArgs {
   int64_t ldb;
   void *C;
   int64_t ldc;
+  // grouped engine: regular slots per 8-tile group in row-sorted order
+  int64_t nreg;
+  const int *g_row, *g_col;
+  const void *g_val;
 };
 
 namespace {
@@ -99,6 +103,77 @@ __global__ void __launch_bounds__(256) tiled_rowmajor_kernel(const TiledArgs a) 
           }
 #pragma unroll
           for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+        }
+      }
+    }
+    if (cur >= 0 && inb) vatomic_add<T, ACC, VB>(C + (int64_t)cur * a.ldc + col, acc);
+  }
+}
+
+// Grouped engine (the slot order of Swift_GPU_4, src/Swift_4.h:6-76): one warp per group of 8
+// tiles (256 slots, the last group shorter), whose slots are stored in row-sorted order; each
+// sub-warp takes an equal share of them, sums each run of equal rows in registers and issues
+// one vector atomic per run -- one per distinct row of the share, where the slot-ordered engine
+// issues one per change of row between neighbouring slots.
+template <class T, class ACC, int VB, int SG>
+__global__ void __launch_bounds__(256) grouped_rowmajor_kernel(const TiledArgs a) {
+  constexpr int G = 32 / SG;
+  constexpr int CW = SG * VB;
+  constexpr int BATCH = 8;
+  const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
+  const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
+  const int64_t grp = (int64_t)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int64_t s0 = grp * 256;
+  if (s0 >= a.nreg) return;
+  const int cnt = (int)(a.nreg - s0 < 256 ? a.nreg - s0 : 256);
+  const int per = (cnt + G - 1) / G;
+  const int lo = sg * per, hi = min(cnt, lo + per);
+  const T *__restrict__ B = static_cast<const T *>(a.B);
+  T *__restrict__ C = static_cast<T *>(a.C);
+  const T *__restrict__ gval = static_cast<const T *>(a.g_val);
+  for (int cbase = 0; cbase < a.N; cbase += CW) {
+    const int col = cbase + sl * VB;
+    const bool inb = col < a.N;
+    int cur = -1;
+    ACC acc[VB];
+#pragma unroll
+    for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+    for (int k0 = lo; k0 < hi; k0 += SG) {
+      const int m = min(SG, hi - k0);  // the same for every lane of the sub-warp
+      int myr = 0, myb = 0;
+      ACC myv = ACC(0);
+      if (sl < m) {
+        const int64_t s = s0 + k0 + sl;
+        myr = __ldg(a.g_row + s);
+        const int c = __ldg(a.g_col + s);
+        myb = a.presorted ? c : __ldg(a.perm + c);
+        myv = (ACC)__ldg(gval + s);
+      }
+      for (int u0 = 0; u0 < m; u0 += BATCH) {
+        ACC b[BATCH][VB];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+          const int brow = __shfl_sync(sgmask, myb, (u0 + u) & (SG - 1), SG);
+          if (inb && u0 + u < m) vload<T, ACC, VB>(B + (int64_t)brow * a.ldb + col, b[u]);
+          else {
+#pragma unroll
+            for (int e = 0; e < VB; ++e) b[u][e] = ACC(0);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+          const int r = __shfl_sync(sgmask, myr, (u0 + u) & (SG - 1), SG);
+          const ACC w = __shfl_sync(sgmask, myv, (u0 + u) & (SG - 1), SG);
+          if (u0 + u < m) {
+            if (r != cur) {
+              if (cur >= 0 && inb) vatomic_add<T, ACC, VB>(C + (int64_t)cur * a.ldc + col, acc);
+              cur = r;
+#pragma unroll
+              for (int e = 0; e < VB; ++e) acc[e] = ACC(0);
+            }
+#pragma unroll
+            for (int e = 0; e < VB; ++e) acc[e] = fma(w, b[u][e], acc[e]);
+          }
         }
       }
     }
@@ -226,7 +301,14 @@ __global__ void __launch_bounds__(256) reside_colmajor_kernel(const TiledArgs a)
 
 template <class T, class ACC, int VB, int SG>
 swift_status launch_rowmajor(const TiledArgs &a, cudaStream_t st) {
-  if (a.nitems > 0) {
+  if (a.g_row) {
+    const int64_t groups = (a.nreg + 255) / 256;
+    if (groups > 0) {
+      const int64_t blocks = (groups * 32 + 255) / 256;
+      grouped_rowmajor_kernel<T, ACC, VB, SG><<<(unsigned)blocks, 256, 0, st>>>(a);
+      SW_CHECK_LAUNCH();
+    }
+  } else if (a.nitems > 0) {
     const int64_t blocks = ((int64_t)a.nitems * 32 + 255) / 256;
     tiled_rowmajor_kernel<T, ACC, VB, SG><<<(unsigned)blocks, 256, 0, st>>>(a);
     SW_CHECK_LAUNCH();
@@ -279,8 +361,9 @@ swift_status zero_dense(void *C, int rows, int N, int64_t ld, swift_layout layou
   return SWIFT_OK;
 }
 
-swift_status run_tiled(const Plan &p, const DenseArgs &d, int reside_variant, cudaStream_t st) {
+swift_status run_tiled(const Plan &p, const DenseArgs &d, int reside_variant, cudaStream_t st, bool grouped) {
   if (d.b_layout != d.c_layout) return SWIFT_ERR_UNSUPPORTED;
+  if (grouped && (d.c_layout != SWIFT_ROW_MAJOR || !p.grouped_built)) return SWIFT_ERR_UNSUPPORTED;
   if (d.dtype == SWIFT_BF16 || d.dtype == SWIFT_F16) return SWIFT_ERR_UNSUPPORTED;
   if ((d.dtype == SWIFT_F64) != (p.val_type == SWIFT_F64)) return SWIFT_ERR_UNSUPPORTED;
   const size_t esz = d.dtype == SWIFT_F64 ? 8 : 4;
@@ -304,6 +387,12 @@ swift_status run_tiled(const Plan &p, const DenseArgs &d, int reside_variant, cu
   a.blkstart = p.blkstart.as<int>();
   a.blkstop = p.blkstop.as<int>();
   a.B = d.B; a.ldb = d.ldb; a.C = d.C; a.ldc = d.ldc;
+  a.nreg = (int64_t)p.tilenum * kTile;
+  if (grouped) {
+    a.g_row = p.g_row.as<int>();
+    a.g_col = p.g_col.as<int>();
+    a.g_val = p.g_val.p;
+  }
   if (!d.b_presorted && !p.perm.p) return SWIFT_ERR_INVALID_ARG;
   if (d.c_layout == SWIFT_COL_MAJOR)
     return d.dtype == SWIFT_F64 ? launch_colmajor<double>(a, st) : launch_colmajor<float>(a, st);

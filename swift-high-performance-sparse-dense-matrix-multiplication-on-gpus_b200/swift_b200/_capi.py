@@ -17,7 +17,7 @@ OK, ERR_INVALID_ARG, ERR_BAD_CSR, ERR_BAD_PERM, ERR_UNSUPPORTED, ERR_CUDA, ERR_A
 F32, F64, BF16, F16 = 0, 1, 2, 3
 ROW_MAJOR, COL_MAJOR = 0, 1
 HOST, DEVICE = 0, 1
-ENGINE_AUTO, ENGINE_TILED, ENGINE_ROWWISE = 0, 1, 2
+ENGINE_AUTO, ENGINE_TILED, ENGINE_ROWWISE, ENGINE_TILED_GROUPED = 0, 1, 2, 3
 
 
 class SwiftError(RuntimeError):

@@ -220,7 +220,8 @@ class Plan:
 
     # ------------------------------------------------------------------ products
     def spmm(self, B, C_out=None, engine="auto", b_presorted=False, layout="row", stream=None):
-        """C = A @ B.  layout 'row' (row-major B/C) or 'col' (column-major, Fortran order)."""
+        """C = A @ B.  layout 'row' (row-major B/C) or 'col' (column-major, Fortran order);
+        engine 'auto', 'rowwise', 'tiled' or 'tiled_grouped' (row-major, FP32/FP64)."""
         torch = _torch()
         lay = capi.ROW_MAJOR if layout == "row" else capi.COL_MAJOR
         N = int(B.shape[1])
@@ -230,7 +231,8 @@ class Plan:
             if lay == capi.COL_MAJOR:
                 C_out = torch.empty((N, self.M), dtype=B.dtype, device=B.device).t()
         _dense(C_out, self.M, N, "C_out", B.dtype)
-        eng = {"auto": capi.ENGINE_AUTO, "tiled": capi.ENGINE_TILED, "rowwise": capi.ENGINE_ROWWISE}[engine]
+        eng = {"auto": capi.ENGINE_AUTO, "tiled": capi.ENGINE_TILED, "rowwise": capi.ENGINE_ROWWISE,
+               "tiled_grouped": capi.ENGINE_TILED_GROUPED}[engine]
         capi.check(capi.lib().swift_spmm(self._h, eng, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, lay), lay,
                                          int(b_presorted), C_out.data_ptr(), _ld(C_out, lay), lay,
                                          _stream_ptr(stream)), "swift_spmm")
@@ -347,7 +349,8 @@ class Plan:
         capi.check(capi.lib().swift_plan_autotune(self._h, N, _dtype_code(B.dtype), B.data_ptr(),
                                                   C_out.data_ptr(), _stream_ptr(stream), C.byref(ms),
                                                   C.byref(eng)), "swift_plan_autotune")
-        return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise"}[eng.value], ms.value
+        return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise",
+                capi.ENGINE_TILED_GROUPED: "tiled_grouped"}[eng.value], ms.value
 
 
 class Batch:

@@ -41,7 +41,7 @@ def test_set_values_equals_fresh_build(dt):
     for k in ("sortval", "reside_val", "sortrowidx", "tile_colidx"):
         assert np.array_equal(ea[k], eb[k]), k
     B = torch.rand((M, 64), dtype=torch.float64 if dt == np.float64 else torch.float32, device="cuda")
-    for eng in ("rowwise", "tiled"):
+    for eng in ("rowwise", "tiled", "tiled_grouped"):
         Cp, Cq = p.spmm(B, engine=eng), q.spmm(B, engine=eng)
         if eng == "rowwise":
             assert torch.equal(Cp, Cq)
@@ -52,6 +52,9 @@ def test_set_values_equals_fresh_build(dt):
     p.set_values(v0)  # host values
     r = Plan.from_csr(rp, ci, v0, (M, M))
     assert torch.equal(p.spmm(B, engine="rowwise"), r.spmm(B, engine="rowwise"))
+    # the grouped engine's slots (built above from v1) follow the values back to v0
+    Cg, Cr = p.spmm(B, engine="tiled_grouped"), r.spmm(B, engine="tiled_grouped")
+    assert (Cg - Cr).abs().max().item() <= 1e-5 * Cr.abs().max().item()
 
 
 @pytest.mark.parametrize("shape", [(40, 30, 0.15, 3), (64, 64, 0.3, 5)])

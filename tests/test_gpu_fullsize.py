@@ -131,7 +131,7 @@ def test_rmat20_spmm_vs_full_swift_cpu(rmat20, dt, N):
     plan = Plan.from_csr(rp, ci, v, (M, K))
     c64 = plan.spmm_f64_reference(B.double()).cpu().numpy()
     assert relerr(c_cpu, c64) <= TOL[dt]  # the FP64 GPU oracle agrees with Swift_cpu
-    for engine in ("rowwise", "tiled", "auto"):
+    for engine in ("rowwise", "tiled", "tiled_grouped", "auto"):
         Cm = plan.spmm(B, engine=engine).cpu().numpy()
         e_ref, e_64 = relerr(Cm, c_cpu), relerr(Cm, c64)
         print(f"N={N} {np.dtype(dt).name} {engine}: vs Swift_cpu {e_ref:.3e}, vs FP64 GPU product {e_64:.3e}")

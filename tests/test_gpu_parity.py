@@ -64,7 +64,7 @@ def test_format_bit_exact_vs_reference_fixture(name, dt):
     pl.close()
 
 
-@pytest.mark.parametrize("engine", ["tiled", "rowwise"])
+@pytest.mark.parametrize("engine", ["tiled", "tiled_grouped", "rowwise"])
 @pytest.mark.parametrize("dt", [np.float32, np.float64])
 @pytest.mark.parametrize("name", golden_io.ALL)
 def test_spmm_matches_swift_cpu(name, dt, engine):
@@ -142,7 +142,7 @@ def test_column_major_small_and_edge_shapes(name, N):
 
 
 @pytest.mark.parametrize("N", [1, 8, 24, 32, 33, 64, 128, 768])
-@pytest.mark.parametrize("engine", ["tiled", "rowwise"])
+@pytest.mark.parametrize("engine", ["tiled", "tiled_grouped", "rowwise"])
 def test_ragged_widths(N, engine):
     M, K, rp, ci = cases.make("rmat12", 0)
     val = gen.uniform_values(int(rp[-1]), 1, np.float32)
