@@ -87,13 +87,23 @@ typedef enum swift_memspace { SWIFT_HOST = 0, SWIFT_DEVICE = 1 } swift_memspace;
  *              sort of src/back_process.h:23-229, run on the GPU when first needed), so equal
  *              rows of a group form one run and take one vector atomic.  Row-major B and C,
  *              FP32 or FP64.
+ *   BAND    -- dense diagonal tiles for matrices whose nonzeros crowd the diagonal: every
+ *              group of 8 rows keeps the columns [8g - W, 8g - W + 8 + 2W) as a dense 8-row
+ *              tile (values only, no indices), multiplied from a TMA-staged B panel with the 8
+ *              rows held in registers; the nonzeros outside the tiles go through the ROWWISE
+ *              walk first.  The half-width W in {3, 7, 15, 31, 47, 63} comes from the plan's
+ *              |col - row| profile (swift_plan_band_profile; 3 when no width pays).  FP32
+ *              plans, F32 / BF16 / F16 row-major B and C with N >= 128, N % 4 == 0, 16-byte
+ *              aligned B, C, ldb and ldc (else SWIFT_ERR_UNSUPPORTED).  The split is built on
+ *              first use.  No counterpart in the reference.
  *   AUTO    -- the autotuned choice for (N, dtype), ROWWISE when no tuning was run and the
  *              layouts allow it. */
 typedef enum swift_engine {
   SWIFT_ENGINE_AUTO = 0,
   SWIFT_ENGINE_TILED = 1,
   SWIFT_ENGINE_ROWWISE = 2,
-  SWIFT_ENGINE_TILED_GROUPED = 3
+  SWIFT_ENGINE_TILED_GROUPED = 3,
+  SWIFT_ENGINE_BAND = 4
 } swift_engine;
 
 typedef struct swift_csr {
@@ -300,6 +310,23 @@ swift_status swift_spmm_noalloc(const swift_plan *plan, int N, swift_dtype dtype
                                 int64_t ldb, void *C, int64_t ldc, swift_stream_t stream);
 
 /* ------------------------------------------------------------------ tuning */
+/* Diagonal profile of A, measured on the GPU once per plan (synchronises `stream` the first
+ * time): hist[d] = nonzeros with |col - row| == d for d = 0..SWIFT_BAND_PROFILE_MAX (hist may
+ * be NULL), and the BAND engine's half-width: the W in {3, 7, 15, 31, 47, 63} with the largest
+ * (nonzeros within distance W) - M * (8 + 2W) / 8 -- the gathers the tiles save against the
+ * dense work they add, a gathered nonzero costing the row walk about eight dense tile
+ * elements -- if that saves at least a twentieth of the nonzeros, else -1.  AUTO's tuner
+ * tries the BAND engine only when the half-width is >= 0.  No counterpart in the reference. */
+#define SWIFT_BAND_PROFILE_MAX 128
+swift_status swift_plan_band_profile(swift_plan *plan, long long *hist, int *half_width,
+                                     swift_stream_t stream);
+
+/* Whether a BAND product's block gave up waiting for its TMA copies (a bounded wait of about
+ * two seconds; the block then leaves its C rows without the tiles' part): *flag = 1 if any did
+ * since the last reset.  Synchronous; reset != 0 clears the flag.  No counterpart in the
+ * reference. */
+swift_status swift_band_timeout_flag(int *flag, int reset);
+
 /* Times the engines and their parameters on this plan for (N, dtype) with CUDA events and
  * stores the fastest as the plan's AUTO choice.  B and C are caller buffers of the right
  * shape (row-major); their contents are overwritten.  best_ms may be NULL. */

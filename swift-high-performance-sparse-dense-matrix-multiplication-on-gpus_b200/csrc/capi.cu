@@ -25,10 +25,11 @@ size_t plan_device_bytes(const Plan &p) {
                           &p.step_tall, &p.step_tile_off, &p.item_tile, &p.tile_colidx,
                           &p.tile_depth, &p.tile_tall, &p.tile_format, &p.sortrowidx, &p.sortval,
                           &p.reside_ptr, &p.reside_row, &p.reside_val, &p.colorblk, &p.blkstart,
-                          &p.blkstop, &p.blkptr, &p.rowcopy_b, &p.rowcopy_c};
+                          &p.blkstop, &p.blkptr, &p.rowcopy_b, &p.rowcopy_c, &p.g_row, &p.g_col,
+                          &p.g_val, &p.band_tiles, &p.band_ptr, &p.band_idx, &p.band_val, &p.band_dst};
   size_t s = 0;
   for (const DevBuf *b : bufs) s += b->bytes;
-  for (const RowLayout *L : {&p.fwd, &p.bwd}) {
+  for (const RowLayout *L : {&p.fwd, &p.bwd, &p.band_rest}) {
     const DevBuf *lb[] = {&L->piece_row, &L->piece_idx, &L->long_first, &L->long_count,
                           &L->long_of_row, &L->counters, &L->scratch, &L->task_row,
                           &L->head_split, &L->tail_split, &L->split_row, &L->split_first,
@@ -260,6 +261,7 @@ swift_status swift_plan_set_values(swift_plan *plan, const void *val, swift_mems
   if (p.nnz > 0)
     SW_CHECK_CUDA(cudaMemcpyAsync(p.val.p, val, p.vsz * (size_t)p.nnz,
                                   mem == SWIFT_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  SW_TRY(band_refill(p, st));  // the band split's tiles and rest take the new values in place
   return refresh_values(p, st);
 }
 
@@ -340,7 +342,8 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
                         (engine == SWIFT_ENGINE_ROWWISE || (engine == SWIFT_ENGINE_AUTO && [&] {
                            std::lock_guard<std::mutex> g(p.mu);
                            auto it = p.tuned.find({N, (int)dtype});
-                           return it == p.tuned.end() || it->second == SWIFT_ENGINE_ROWWISE;
+                           return it == p.tuned.end() || it->second == SWIFT_ENGINE_ROWWISE ||
+                                  it->second == SWIFT_ENGINE_BAND;
                          }()));
   if (via_rows) {
     const size_t esz = dtype == SWIFT_F64 ? 8 : (dtype == SWIFT_F32 ? 4 : 2);
@@ -370,7 +373,9 @@ swift_status swift_spmm(const swift_plan *plan, swift_engine engine, int N, swif
     std::lock_guard<std::mutex> g(p.mu);
     auto it = p.tuned.find({N, (int)dtype});
     if (it != p.tuned.end() && (it->second == SWIFT_ENGINE_TILED || row_ok)) engine = it->second;
+    if (engine == SWIFT_ENGINE_BAND && !band_operands_ok(p, d)) engine = SWIFT_ENGINE_ROWWISE;
   }
+  if (engine == SWIFT_ENGINE_BAND) return run_band(p, d, merge_opts_for(p, N, dtype), st);
   if (engine == SWIFT_ENGINE_ROWWISE) {
     if (!row_ok) return SWIFT_ERR_UNSUPPORTED;
     if (p.M == 0) return SWIFT_OK;
@@ -525,6 +530,14 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
     cands.push_back({SWIFT_ENGINE_TILED, MergeOpts{}});
     cands.push_back({SWIFT_ENGINE_TILED_GROUPED, MergeOpts{}});
   }
+  if (p.has_csr && p.val_type == SWIFT_F32 && dtype != SWIFT_F64 && N >= 128 && N % 4 == 0) {
+    int w = -1;
+    {
+      std::lock_guard<std::mutex> g(p.mu);
+      if (band_profile(p, st) == SWIFT_OK) w = p.band_w;
+    }
+    if (w >= 0) cands.push_back({SWIFT_ENGINE_BAND, MergeOpts{}});
+  }
   if (p.has_csr) {
     // task size (the work-balance grain) x (loads in flight, vector bytes, kernel variant)
     const int shapes[][3] = {{4, 16, 1}, {8, 16, 1}, {4, 32, 1}, {4, 16, 2}, {4, 32, 2}};
@@ -585,6 +598,23 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
   if (best_engine) *best_engine = win.eng;
   return SWIFT_OK;
 }
+
+swift_status swift_plan_band_profile(swift_plan *plan, long long *hist, int *half_width,
+                                     swift_stream_t stream) {
+  if (!plan) return SWIFT_ERR_INVALID_ARG;
+  Plan &p = plan->p;
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  cudaStream_t st = S(stream);
+  UseNote use_note{p, st};
+  std::lock_guard<std::mutex> g(p.mu);
+  SW_TRY(band_profile(p, st));
+  if (hist)
+    for (int d = 0; d <= SWIFT_BAND_PROFILE_MAX; ++d) hist[d] = p.band_hist[d];
+  if (half_width) *half_width = p.band_w;
+  return SWIFT_OK;
+}
+
+swift_status swift_band_timeout_flag(int *flag, int reset) { return band_timeout_flag(flag, reset); }
 
 swift_status swift_plan_set_rowwise_params(swift_plan *plan, int task_size, int loads_in_flight,
                                            int vector_bytes, int kernel) {

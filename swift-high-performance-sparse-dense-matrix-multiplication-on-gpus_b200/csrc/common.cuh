@@ -201,6 +201,14 @@ struct Plan {
   // sorted column and value per sorted slot (built on first use; new values invalidate it)
   DevBuf g_row, g_col, g_val;
   bool grouped_built = false;
+  // band engine (spmm_band.cu): |col - row| profile, the chosen half-width (-2 not profiled
+  // yet, -1 no width pays), and the split of A into dense diagonal tiles + the rest (built on
+  // first use; new values are scattered through band_dst)
+  int band_w = -2, band_used_w = -1, band_rest_nnz = 0;
+  long long band_hist[129] = {};
+  bool band_built = false;
+  DevBuf band_tiles, band_ptr, band_idx, band_val, band_dst;
+  RowLayout band_rest;
   std::mutex mu;  // guards lazily built layouts and scratch growth
   // Streams this plan's work was enqueued on, each with an event recorded after its latest
   // call, so that destroying the plan waits for its own work only.  Work captured into a CUDA
@@ -291,6 +299,13 @@ swift_status run_tiled(const Plan &p, const DenseArgs &a, int reside_variant, cu
 // leaves them (src/back_process.h:23-229); both null to sort p.sortrowidx here.  A vpos that is
 // not a permutation of each group returns SWIFT_ERR_INVALID_ARG.
 swift_status build_grouped(Plan &p, const int *keys, const int *vpos, cudaStream_t st);
+
+// band engine (spmm_band.cu)
+swift_status band_profile(Plan &p, cudaStream_t st);  // p.mu held
+swift_status band_refill(Plan &p, cudaStream_t st);   // p.mu held
+bool band_operands_ok(const Plan &p, const DenseArgs &d);
+swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStream_t st);
+swift_status band_timeout_flag(int *flag, int reset);
 swift_status run_rowwise(Plan &p, RowLayout &L, const DenseArgs &a, cudaStream_t st);
 swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpts &o,
                        cudaStream_t st);

@@ -331,7 +331,11 @@ swift_status check_slide(const SLIDE *m, int variant, int M, int K) {
     set_last_error("slide_matrix", what);
     return SWIFT_ERR_INVALID_ARG;
   };
-  if (m->tilenum < 0 || m->reside_col < 0 || m->reside_nnz < 0 || m->numblk < 0) return bad("negative size");
+  // Swift_gpu1 runs before balance() in the reference's driver (test/k-32/FP32/main.cu:359-382),
+  // so its slide_matrix still holds whatever malloc left in numblk/colorblk: variant 1 reads
+  // neither field.
+  if (m->tilenum < 0 || m->reside_col < 0 || m->reside_nnz < 0 || (variant != 1 && m->numblk < 0))
+    return bad("negative size");
   const size_t nreg = (size_t)m->tilenum * kTile;
   if (m->tilenum > 0 && (!m->tile_colidx || !m->sortrowidx || !m->sortval)) return bad("missing tile arrays");
   for (int t = 0; t < m->tilenum; ++t)

@@ -1,0 +1,455 @@
+// spmm_band.cu -- dense diagonal tiles (the band engine).
+//
+// Matrices whose nonzeros crowd the diagonal (banded stencils, the |i-j| < 32 band of the
+// precision workload) waste the row walk's per-nonzero B-row gather: neighbouring rows gather
+// almost the same B rows.  The band engine splits A once per plan:
+//   * tiles: for every 8-row group g, a dense 8 x TW tile of the columns
+//     [8g - W, 8g - W + TW), TW = 8 + 2W rounded up to 4 (values only, zeros where A has none);
+//   * rest:  the nonzeros outside their group's tile, as a CSR operand for the row walk.
+// A product runs the row walk over the rest (writing every C row), then the tile kernel adds
+// the tiles' product: one block per 64 rows x 128 columns stages the B rows its tiles touch
+// (64 + TW - 8 rows) in shared memory with one TMA tile load and the block's tile values with
+// one bulk copy; each warp keeps the 8 x 128 slice of its C rows in registers, so every B row
+// read from shared memory feeds eight rows' FMAs (a loaded B vector is used 8 times, a loaded
+// tile vector 4 times).
+//
+// The half-width W is chosen from the plan's distance profile (nonzeros per |col - row|, one
+// GPU pass): the W that saves the most gathered rows for the dense work it adds, if it saves at
+// least a twentieth of the walk's gathers.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "vec.cuh"
+
+namespace swift {
+
+namespace {
+
+constexpr int kGroup = 8;          // rows per tile (one warp)
+constexpr int kCtaRows = 64;       // rows per block (eight warps)
+constexpr int kSlice = 128;        // dense columns per block (32 lanes x 4)
+constexpr int kMaxDist = 128;      // |col - row| profiled up to this distance
+constexpr int kWidths[] = {3, 7, 15, 31, 47, 63};
+
+__device__ int g_band_timeout;     // set when a block's copy wait ran out
+
+constexpr int tile_width(int w) { return (kGroup + 2 * w + 3) / 4 * 4; }
+constexpr int panel_rows(int tw) { return kCtaRows - kGroup + tw; }
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait on phase `parity` of an mbarrier: about two seconds of SM clock at most.
+__device__ __forceinline__ bool wait_phase(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > 4000000000LL) return false;
+  }
+}
+
+// |col - row| histogram (distances above kMaxDist are not counted).
+__global__ void band_profile_kernel(const int *__restrict__ rowptr, const int *__restrict__ colidx, int M,
+                                    unsigned long long *__restrict__ hist) {
+  __shared__ unsigned int sh[kMaxDist + 1];
+  for (int t = threadIdx.x; t <= kMaxDist; t += blockDim.x) sh[t] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < M; i += (gridDim.x * blockDim.x) >> 5) {
+    const int e1 = __ldg(rowptr + i + 1);
+    for (int e = __ldg(rowptr + i) + lane; e < e1; e += 32) {
+      const int d = abs(__ldg(colidx + e) - i);
+      if (d <= kMaxDist) atomicAdd(&sh[d], 1u);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t <= kMaxDist; t += blockDim.x)
+    if (sh[t]) atomicAdd(hist + t, (unsigned long long)sh[t]);
+}
+
+// Per row: nonzeros outside the row's group tile.
+__global__ void band_count_kernel(const int *__restrict__ rowptr, const int *__restrict__ colidx, int M, int W,
+                                  int TW, int *__restrict__ rest_cnt) {
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < M; i += (gridDim.x * blockDim.x) >> 5) {
+    const int c0 = (i & ~(kGroup - 1)) - W;
+    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
+    int cnt = 0;
+    for (int b = e0; b < e1; b += 32) {
+      const int e = b + lane;
+      bool out = false;
+      if (e < e1) {
+        const int j = __ldg(colidx + e);
+        out = j < c0 || j >= c0 + TW;
+      }
+      cnt += __popc(__ballot_sync(0xffffffffu, out));
+    }
+    if (lane == 0) rest_cnt[i] = cnt;
+  }
+}
+
+// Per row: tile entries into the tiles, the others (in row order) into the rest CSR; dst[e]
+// records where nonzero e went (>= 0: rest position, < 0: -1 - tile position) for value updates.
+template <class TV>
+__global__ void band_split_kernel(const int *__restrict__ rowptr, const int *__restrict__ colidx,
+                                  const TV *__restrict__ val, int M, int W, int TW, const int *__restrict__ rest_ptr,
+                                  int *__restrict__ rest_idx, TV *__restrict__ rest_val, float *__restrict__ tiles,
+                                  int *__restrict__ dst) {
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < M; i += (gridDim.x * blockDim.x) >> 5) {
+    const int c0 = (i & ~(kGroup - 1)) - W;
+    const int e0 = __ldg(rowptr + i), e1 = __ldg(rowptr + i + 1);
+    int base = __ldg(rest_ptr + i);
+    for (int b = e0; b < e1; b += 32) {
+      const int e = b + lane;
+      bool out = false;
+      int j = 0;
+      if (e < e1) {
+        j = __ldg(colidx + e);
+        out = j < c0 || j >= c0 + TW;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, out);
+      if (e < e1) {
+        if (out) {
+          const int pos = base + __popc(m & below);
+          rest_idx[pos] = j;
+          rest_val[pos] = val[e];
+          dst[e] = pos;
+        } else {
+          const int tpos = i * TW + (j - c0);
+          tiles[tpos] = (float)val[e];
+          dst[e] = -1 - tpos;
+        }
+      }
+      base += __popc(m);
+    }
+  }
+}
+
+// New values for the fixed pattern: scatter through dst.
+template <class TV>
+__global__ void band_refill_kernel(const TV *__restrict__ val, int64_t nnz, const int *__restrict__ dst,
+                                   TV *__restrict__ rest_val, float *__restrict__ tiles) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int d = dst[e];
+    if (d >= 0) rest_val[d] = val[e];
+    else tiles[-1 - d] = (float)val[e];
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void load4(const T *p, float (&o)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 f = *reinterpret_cast<const float4 *>(p);
+    o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+  } else {
+    const uint2 u = *reinterpret_cast<const uint2 *>(p);
+    const float2 a = unpack2<T>(u.x), b = unpack2<T>(u.y);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void store4(T *p, const float (&v)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    __stcs(reinterpret_cast<float4 *>(p), make_float4(v[0], v[1], v[2], v[3]));
+  } else {
+    T h[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) h[k] = from_acc<T>(v[k]);
+    *reinterpret_cast<uint2 *>(p) = *reinterpret_cast<const uint2 *>(h);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void load4_global(const T *p, float (&o)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 f = __ldcs(reinterpret_cast<const float4 *>(p));
+    o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+  } else {
+    const uint2 u = __ldcs(reinterpret_cast<const uint2 *>(p));
+    const float2 a = unpack2<T>(u.x), b = unpack2<T>(u.y);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  }
+}
+
+// C[rows of this block, this 128-column slice] += tiles x B.  Shared memory: the B panel
+// (panel_rows(TW) x 128 elements, rows i0 - W ..; rows outside B are zero-filled by the TMA
+// unit), the block's 64 x TW tile values, one mbarrier.
+template <class T, int TW, int MINB>
+__global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_constant__ CUtensorMap bmap,
+                                                              const float *__restrict__ tiles, int M, int N, int W,
+                                                              T *__restrict__ C, int64_t ldc) {
+  constexpr int PR = panel_rows(TW);
+  constexpr uint32_t PANEL_BYTES = (uint32_t)PR * kSlice * sizeof(T);
+  constexpr uint32_t VAL_BYTES = (uint32_t)kCtaRows * TW * 4;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const T *Bs = reinterpret_cast<const T *>(sm);
+  const float *Es = reinterpret_cast<const float *>(sm + PANEL_BYTES);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + PANEL_BYTES + VAL_BYTES);
+  const int i0 = blockIdx.x * kCtaRows, col0 = blockIdx.y * kSlice;
+  const uint32_t b = smem_addr(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(PANEL_BYTES + VAL_BYTES) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(Bs)), "l"(reinterpret_cast<uint64_t>(&bmap)), "r"(col0), "r"(i0 - W), "r"(b)
+        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(Es)), "l"(tiles + (size_t)i0 * TW), "r"(VAL_BYTES), "r"(b)
+                 : "memory");
+  }
+  __syncthreads();
+  if (!wait_phase(b, 0)) {
+    if (threadIdx.x == 0) atomicExch(&g_band_timeout, 1);
+    wait_phase(b, 0);  // give copies still in flight a second bounded chance before leaving
+    return;
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float acc[kGroup][4];
+#pragma unroll
+  for (int r = 0; r < kGroup; ++r)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[r][k] = 0.f;
+  const T *Bw = Bs + (size_t)(kGroup * w) * kSlice + lane * 4;  // panel row of tile column 0
+  const float *E = Es + (size_t)(kGroup * w) * TW;
+#pragma unroll 2
+  for (int c = 0; c < TW; c += 4) {
+    float bv[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) load4<T>(Bw + (size_t)(c + q) * kSlice, bv[q]);
+#pragma unroll
+    for (int r = 0; r < kGroup; ++r) {
+      const float4 v = *reinterpret_cast<const float4 *>(E + r * TW + c);
+      fma_vec<float, 4>(acc[r], v.x, bv[0]);
+      fma_vec<float, 4>(acc[r], v.y, bv[1]);
+      fma_vec<float, 4>(acc[r], v.z, bv[2]);
+      fma_vec<float, 4>(acc[r], v.w, bv[3]);
+    }
+  }
+  const int col = col0 + lane * 4;
+  if (col < N) {
+#pragma unroll
+    for (int r = 0; r < kGroup; ++r) {
+      const int row = i0 + kGroup * w + r;
+      if (row < M) {
+        T *cp = C + (int64_t)row * ldc + col;
+        float old[4];
+        load4_global<T>(cp, old);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[r][k] += old[k];
+        store4<T>(cp, acc[r]);
+      }
+    }
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+template <class T, int TW>
+swift_status launch_tile(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
+                         cudaStream_t st) {
+  constexpr size_t smem = (size_t)panel_rows(TW) * kSlice * sizeof(T) + (size_t)kCtaRows * TW * 4 + 16;
+  constexpr int minb = smem * 2 <= 220 * 1024 ? 2 : 1;
+  auto k = band_tile_kernel<T, TW, minb>;
+  SW_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const dim3 grid((unsigned)((M + kCtaRows - 1) / kCtaRows), (unsigned)((N + kSlice - 1) / kSlice));
+  k<<<grid, 256, smem, st>>>(map, tiles, M, N, W, static_cast<T *>(C), ldc);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+template <class T>
+swift_status launch_tile_w(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
+                           cudaStream_t st) {
+  switch (W) {
+    case 3: return launch_tile<T, tile_width(3)>(map, tiles, M, N, W, C, ldc, st);
+    case 7: return launch_tile<T, tile_width(7)>(map, tiles, M, N, W, C, ldc, st);
+    case 15: return launch_tile<T, tile_width(15)>(map, tiles, M, N, W, C, ldc, st);
+    case 31: return launch_tile<T, tile_width(31)>(map, tiles, M, N, W, C, ldc, st);
+    case 47: return launch_tile<T, tile_width(47)>(map, tiles, M, N, W, C, ldc, st);
+    case 63: return launch_tile<T, tile_width(63)>(map, tiles, M, N, W, C, ldc, st);
+  }
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
+}  // namespace
+
+// Distance profile and the half-width choice (p.mu held).
+swift_status band_profile(Plan &p, cudaStream_t st) {
+  if (p.band_w != -2) return SWIFT_OK;
+  if (!p.has_csr) return SWIFT_ERR_UNSUPPORTED;
+  TmpBuf h;
+  SW_TRY(h.alloc(sizeof(unsigned long long) * (kMaxDist + 1), st));
+  SW_CHECK_CUDA(cudaMemsetAsync(h.p, 0, sizeof(unsigned long long) * (kMaxDist + 1), st));
+  if (p.M > 0) {
+    const int grid = std::max(1, std::min((p.M + 7) / 8, p.sm_count * 8));
+    band_profile_kernel<<<grid, 256, 0, st>>>(p.rowptr.as<int>(), p.colidx.as<int>(), p.M,
+                                              static_cast<unsigned long long *>(h.p));
+    SW_CHECK_LAUNCH();
+  }
+  unsigned long long hh[kMaxDist + 1];
+  SW_CHECK_CUDA(cudaMemcpyAsync(hh, h.p, sizeof(hh), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  for (int d = 0; d <= kMaxDist; ++d) p.band_hist[d] = (long long)hh[d];
+  // A gathered nonzero costs the row walk about eight times what one dense tile element costs
+  // the tile kernel (measured: 39 ps per FP32 nonzero at N = 128 against about 4 ps per tile
+  // element); pick the width with the largest saving, if it saves a twentieth of the gathers.
+  double best = 0.05 * (double)p.nnz;
+  int bw = -1;
+  for (int w : kWidths) {
+    long long in = 0;
+    for (int d = 0; d <= w; ++d) in += p.band_hist[d];
+    const double gain = (double)in - (double)p.M * tile_width(w) / 8.0;
+    if (gain > best && (int64_t)((p.M + kCtaRows - 1) / kCtaRows) * kCtaRows * tile_width(w) < INT32_MAX) {
+      best = gain;
+      bw = w;
+    }
+  }
+  p.band_w = bw;
+  return SWIFT_OK;
+}
+
+// Splits A into tiles + rest for half-width W (p.mu held).
+static swift_status band_build(Plan &p, int W, cudaStream_t st) {
+  const int TW = tile_width(W);
+  const int64_t rows_pad = (int64_t)((p.M + kCtaRows - 1) / kCtaRows) * kCtaRows;
+  if (rows_pad * TW >= INT32_MAX) return SWIFT_ERR_OVERFLOW;
+  p.band_built = false;
+  SW_TRY(p.band_tiles.alloc(sizeof(float) * (size_t)std::max<int64_t>(rows_pad * TW, 1)));
+  SW_CHECK_CUDA(cudaMemsetAsync(p.band_tiles.p, 0, p.band_tiles.bytes, st));
+  SW_TRY(p.band_ptr.alloc(sizeof(int) * ((size_t)p.M + 1)));
+  SW_TRY(p.band_dst.alloc(sizeof(int) * (size_t)std::max(p.nnz, 1)));
+  const int grid = std::max(1, std::min((p.M + 7) / 8, p.sm_count * 16));
+  if (p.M > 0) {
+    band_count_kernel<<<grid, 256, 0, st>>>(p.rowptr.as<int>(), p.colidx.as<int>(), p.M, W, TW, p.band_ptr.as<int>());
+    SW_CHECK_LAUNCH();
+  }
+  SW_TRY(scan_exclusive_i32(p.band_ptr.as<int>(), p.band_ptr.as<int>(), p.M, st));
+  int rest = 0;
+  SW_CHECK_CUDA(cudaMemcpyAsync(&rest, p.band_ptr.as<int>() + p.M, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SW_CHECK_CUDA(cudaStreamSynchronize(st));
+  SW_TRY(p.band_idx.alloc(sizeof(int) * (size_t)std::max(rest, 1)));
+  SW_TRY(p.band_val.alloc(p.vsz * (size_t)std::max(rest, 1)));
+  if (p.M > 0) {
+    if (p.val_type == SWIFT_F64)
+      band_split_kernel<double><<<grid, 256, 0, st>>>(p.rowptr.as<int>(), p.colidx.as<int>(), p.val.as<double>(), p.M, W,
+                                                      TW, p.band_ptr.as<int>(), p.band_idx.as<int>(),
+                                                      p.band_val.as<double>(), p.band_tiles.as<float>(),
+                                                      p.band_dst.as<int>());
+    else
+      band_split_kernel<float><<<grid, 256, 0, st>>>(p.rowptr.as<int>(), p.colidx.as<int>(), p.val.as<float>(), p.M, W,
+                                                     TW, p.band_ptr.as<int>(), p.band_idx.as<int>(),
+                                                     p.band_val.as<float>(), p.band_tiles.as<float>(),
+                                                     p.band_dst.as<int>());
+    SW_CHECK_LAUNCH();
+  }
+  // the rest as a row-walk operand (merge tasks are built on its first product)
+  RowLayout &L = p.band_rest;
+  L = RowLayout();
+  L.rows = p.M; L.cols = p.K; L.nnz = rest;
+  L.ptr = p.band_ptr.as<int>(); L.idx = p.band_idx.as<int>(); L.val = p.band_val.p; L.out_row = nullptr;
+  p.band_rest_nnz = rest;
+  p.band_used_w = W;
+  p.band_built = true;
+  return SWIFT_OK;
+}
+
+swift_status band_refill(Plan &p, cudaStream_t st) {
+  if (!p.band_built || p.nnz == 0) return SWIFT_OK;
+  const int grid = (int)std::min<int64_t>(((int64_t)p.nnz + 255) / 256, (int64_t)p.sm_count * 16);
+  if (p.val_type == SWIFT_F64)
+    band_refill_kernel<double><<<grid, 256, 0, st>>>(p.val.as<double>(), p.nnz, p.band_dst.as<int>(),
+                                                     p.band_val.as<double>(), p.band_tiles.as<float>());
+  else
+    band_refill_kernel<float><<<grid, 256, 0, st>>>(p.val.as<float>(), p.nnz, p.band_dst.as<int>(),
+                                                    p.band_val.as<float>(), p.band_tiles.as<float>());
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+bool band_operands_ok(const Plan &p, const DenseArgs &d) {
+  if (!p.has_csr || p.val_type != SWIFT_F32) return false;
+  if (d.dtype != SWIFT_F32 && d.dtype != SWIFT_BF16 && d.dtype != SWIFT_F16) return false;
+  if (d.b_layout != SWIFT_ROW_MAJOR || d.c_layout != SWIFT_ROW_MAJOR || d.b_presorted) return false;
+  if (d.b_scale || d.c_scale) return false;
+  const size_t esz = d.dtype == SWIFT_F32 ? 4 : 2;
+  if (d.N < kSlice || d.N % 4 != 0) return false;
+  if ((uintptr_t)d.B % 16 != 0 || (d.ldb * (int64_t)esz) % 16 != 0) return false;
+  if ((uintptr_t)d.C % 16 != 0 || (d.ldc * (int64_t)esz) % 16 != 0) return false;
+  return true;
+}
+
+swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStream_t st) {
+  if (!band_operands_ok(p, d)) return SWIFT_ERR_UNSUPPORTED;
+  if (p.M == 0 || d.N == 0) return SWIFT_OK;
+  int W = 0;
+  {
+    std::lock_guard<std::mutex> g(p.mu);
+    SW_TRY(band_profile(p, st));
+    W = p.band_w >= 0 ? p.band_w : kWidths[0];
+    if (!p.band_built || p.band_used_w != W) SW_TRY(band_build(p, W, st));
+  }
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) {
+    set_last_error("cuTensorMapEncodeTiled", "driver entry point not available");
+    return SWIFT_ERR_CUDA;
+  }
+  const size_t esz = d.dtype == SWIFT_F32 ? 4 : 2;
+  const int TW = tile_width(W);
+  CUtensorMap map;
+  cuuint64_t dims[2] = {(cuuint64_t)d.N, (cuuint64_t)std::max(p.K, 1)};
+  cuuint64_t strides[1] = {(cuuint64_t)(d.ldb * (int64_t)esz)};
+  cuuint32_t box[2] = {(cuuint32_t)kSlice, (cuuint32_t)panel_rows(TW)};
+  cuuint32_t es[2] = {1, 1};
+  const CUtensorMapDataType dt = d.dtype == SWIFT_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : d.dtype == SWIFT_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  const CUresult cr = enc(&map, dt, 2, const_cast<void *>(d.B), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled", "B cannot be described as a TMA tensor");
+    return SWIFT_ERR_UNSUPPORTED;
+  }
+  // the rest first: the row walk writes every C row (zeros where a row has no rest nonzeros)
+  SW_TRY(run_merge(p, p.band_rest, d, o, st));
+  const float *tiles = p.band_tiles.as<float>();
+  switch (d.dtype) {
+    case SWIFT_F32: return launch_tile_w<float>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
+    case SWIFT_BF16: return launch_tile_w<__nv_bfloat16>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
+    case SWIFT_F16: return launch_tile_w<__half>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
+    default: return SWIFT_ERR_UNSUPPORTED;
+  }
+}
+
+swift_status band_timeout_flag(int *flag, int reset) {
+  int v = 0;
+  SW_CHECK_CUDA(cudaMemcpyFromSymbol(&v, g_band_timeout, sizeof(int)));
+  if (reset && v) {
+    const int z = 0;
+    SW_CHECK_CUDA(cudaMemcpyToSymbol(g_band_timeout, &z, sizeof(int)));
+  }
+  if (flag) *flag = v;
+  return SWIFT_OK;
+}
+
+}  // namespace swift

@@ -17,7 +17,8 @@ OK, ERR_INVALID_ARG, ERR_BAD_CSR, ERR_BAD_PERM, ERR_UNSUPPORTED, ERR_CUDA, ERR_A
 F32, F64, BF16, F16 = 0, 1, 2, 3
 ROW_MAJOR, COL_MAJOR = 0, 1
 HOST, DEVICE = 0, 1
-ENGINE_AUTO, ENGINE_TILED, ENGINE_ROWWISE, ENGINE_TILED_GROUPED = 0, 1, 2, 3
+ENGINE_AUTO, ENGINE_TILED, ENGINE_ROWWISE, ENGINE_TILED_GROUPED, ENGINE_BAND = 0, 1, 2, 3, 4
+BAND_PROFILE_MAX = 128
 
 
 class SwiftError(RuntimeError):
@@ -125,6 +126,8 @@ _SIGS = [
     ("swift_plan_get_stats", C.c_int, [_P, C.POINTER(swift_plan_stats)]),
     ("swift_plan_set_values", C.c_int, [_P, _P, C.c_int, _P]),
     ("swift_plan_is_symmetric", C.c_int, [_P, C.POINTER(C.c_int), _P]),
+    ("swift_plan_band_profile", C.c_int, [_P, _P, C.POINTER(C.c_int), _P]),
+    ("swift_band_timeout_flag", C.c_int, [C.POINTER(C.c_int), C.c_int]),
     ("swift_plan_set_symmetry", C.c_int, [_P, C.c_int]),
     ("swift_plan_export_f32", C.c_int, [_P, C.POINTER(swift_slide_matrix_f32), C.c_int, C.POINTER(C.c_float)]),
     ("swift_plan_export_f64", C.c_int, [_P, C.POINTER(swift_slide_matrix_f64), C.c_int, C.POINTER(C.c_float)]),

