@@ -7,11 +7,12 @@
 //     [8g - W, 8g - W + TW), TW = 8 + 2W rounded up to 4 (values only, zeros where A has none);
 //   * rest:  the nonzeros outside their group's tile, as a CSR operand for the row walk.
 // A product runs the row walk over the rest (writing every C row), then the tile kernel adds
-// the tiles' product: one block per 64 rows x 128 columns stages the B rows its tiles touch
-// (64 + TW - 8 rows) in shared memory with one TMA tile load and the block's tile values with
-// one bulk copy; each warp keeps the 8 x 128 slice of its C rows in registers, so every B row
-// read from shared memory feeds eight rows' FMAs (a loaded B vector is used 8 times, a loaded
-// tile vector 4 times).
+// the tiles' product: persistent blocks, each over a contiguous range of 64-row groups and one
+// 128-column slice, keep the B rows their tiles touch in a shared-memory ring of 64-row chunks
+// filled by TMA tile loads one group ahead (consecutive groups share all but 64 of those rows),
+// with the groups' tile values double-buffered by bulk copies; each warp keeps the 8 x 128
+// slice of its C rows in registers, so every B row read from shared memory feeds eight rows'
+// FMAs (a loaded B vector is used 8 times, a loaded tile vector 4 times).
 //
 // The half-width W is chosen from the plan's distance profile (nonzeros per |col - row|, one
 // GPU pass): the W that saves the most gathered rows for the dense work it adds, if it saves at
@@ -31,6 +32,7 @@ namespace {
 constexpr int kGroup = 8;          // rows per tile (one warp)
 constexpr int kCtaRows = 64;       // rows per block (eight warps)
 constexpr int kSlice = 128;        // dense columns per block (32 lanes x 4)
+constexpr int kChunk = 64;         // B rows per TMA load (one ring slot)
 constexpr int kMaxDist = 128;      // |col - row| profiled up to this distance
 constexpr int kWidths[] = {3, 7, 15, 31, 47, 63};
 
@@ -167,87 +169,157 @@ __device__ __forceinline__ void store4(T *p, const float (&v)[4]) {
   }
 }
 
+// Four consecutive C elements held in their storage type (streaming load, evict-first).
 template <class T>
-__device__ __forceinline__ void load4_global(const T *p, float (&o)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 f = __ldcs(reinterpret_cast<const float4 *>(p));
-    o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
-  } else {
-    const uint2 u = __ldcs(reinterpret_cast<const uint2 *>(p));
-    const float2 a = unpack2<T>(u.x), b = unpack2<T>(u.y);
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+struct Packed4 {
+  uint32_t u[sizeof(T)];  // 4 x 4 bytes (FP32) or 2 x 4 bytes (16-bit)
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int i = 0; i < (int)sizeof(T); ++i) u[i] = 0u;
   }
-}
+  __device__ __forceinline__ void load_stream(const T *p) {
+    if constexpr (sizeof(T) == 4) {
+      const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(p));
+      u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w;
+    } else {
+      const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(p));
+      u[0] = q.x; u[1] = q.y;
+    }
+  }
+  __device__ __forceinline__ void unpack(float (&o)[4]) const {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) o[i] = __uint_as_float(u[i]);
+    } else {
+      const float2 a = unpack2<T>(u[0]), b = unpack2<T>(u[1]);
+      o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+  }
+};
 
-// C[rows of this block, this 128-column slice] += tiles x B.  Shared memory: the B panel
-// (panel_rows(TW) x 128 elements, rows i0 - W ..; rows outside B are zero-filled by the TMA
-// unit), the block's 64 x TW tile values, one mbarrier.
+// C[rows, this 128-column slice] += tiles x B, one persistent block per contiguous range of
+// 64-row groups.  The B rows a group's tiles touch (64 + TW - 8 of them, starting W rows above
+// the group) overlap the next group's by TW - 8 rows, so B lives in a ring of 64-row chunks:
+// each group adds one chunk.  Chunk c holds B rows [rbase + 64c, rbase + 64c + 64) in slot
+// c % NR, NR = (chunks one group touches) + 1, so the chunk of the group after next loads while
+// this group computes; the groups' tile values are double-buffered the same way.  TMA tile
+// loads fill the ring (rows outside B are zero-filled), bulk copies the values, one mbarrier
+// per slot.  The old C rows (the rest walk's result) are loaded into registers before the
+// waits.  Waits are bounded; a block that gives up sets g_band_timeout and leaves.
 template <class T, int TW, int MINB>
 __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_constant__ CUtensorMap bmap,
                                                               const float *__restrict__ tiles, int M, int N, int W,
-                                                              T *__restrict__ C, int64_t ldc) {
+                                                              int ngroups, int per_block, T *__restrict__ C,
+                                                              int64_t ldc) {
   constexpr int PR = panel_rows(TW);
-  constexpr uint32_t PANEL_BYTES = (uint32_t)PR * kSlice * sizeof(T);
+  constexpr int NCH = (PR + kChunk - 1) / kChunk;
+  constexpr int NR = NCH + 1;
+  constexpr int RING_ROWS = NR * kChunk;
+  constexpr uint32_t CHUNK_BYTES = (uint32_t)kChunk * kSlice * sizeof(T);
   constexpr uint32_t VAL_BYTES = (uint32_t)kCtaRows * TW * 4;
   extern __shared__ __align__(1024) unsigned char sm[];
-  const T *Bs = reinterpret_cast<const T *>(sm);
-  const float *Es = reinterpret_cast<const float *>(sm + PANEL_BYTES);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + PANEL_BYTES + VAL_BYTES);
-  const int i0 = blockIdx.x * kCtaRows, col0 = blockIdx.y * kSlice;
-  const uint32_t b = smem_addr(bar);
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(PANEL_BYTES + VAL_BYTES) : "memory");
+  T *ring = reinterpret_cast<T *>(sm);
+  float *vals = reinterpret_cast<float *>(sm + NR * CHUNK_BYTES);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NR * CHUNK_BYTES + 2 * VAL_BYTES);  // NR chunks, 2 values
+  const int g0 = blockIdx.x * per_block;
+  const int g1 = min(g0 + per_block, ngroups);
+  if (g0 >= g1) return;
+  const int nb = g1 - g0, nchunks = nb - 1 + NCH;
+  const int col0 = blockIdx.y * kSlice;
+  const int rbase = g0 * kCtaRows - W;
+  int issued_chunks = 0, issued_vals = 0;  // producer (thread 0) state
+  auto issue_chunk = [&](int c) {
+    const uint32_t b = smem_addr(bar + c % NR);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(CHUNK_BYTES) : "memory");
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-        ::"r"(smem_addr(Bs)), "l"(reinterpret_cast<uint64_t>(&bmap)), "r"(col0), "r"(i0 - W), "r"(b)
+        ::"r"(smem_addr(ring + (size_t)(c % NR) * kChunk * kSlice)), "l"(reinterpret_cast<uint64_t>(&bmap)),
+        "r"(col0), "r"(rbase + kChunk * c), "r"(b)
         : "memory");
+    issued_chunks = c + 1;
+  };
+  auto issue_vals = [&](int k) {
+    const uint32_t b = smem_addr(bar + NR + (k & 1));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(VAL_BYTES) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_addr(Es)), "l"(tiles + (size_t)i0 * TW), "r"(VAL_BYTES), "r"(b)
+                 ::"r"(smem_addr(vals + (size_t)(k & 1) * kCtaRows * TW)),
+                 "l"(tiles + (size_t)(g0 + k) * kCtaRows * TW), "r"(VAL_BYTES), "r"(b)
                  : "memory");
+    issued_vals = k + 1;
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NR + 2; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar + s)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int c = 0; c < NR && c < nchunks; ++c) issue_chunk(c);
+    for (int k = 0; k < 2 && k < nb; ++k) issue_vals(k);
   }
   __syncthreads();
-  if (!wait_phase(b, 0)) {
-    if (threadIdx.x == 0) atomicExch(&g_band_timeout, 1);
-    wait_phase(b, 0);  // give copies still in flight a second bounded chance before leaving
-    return;
-  }
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float acc[kGroup][4];
-#pragma unroll
-  for (int r = 0; r < kGroup; ++r)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc[r][k] = 0.f;
-  const T *Bw = Bs + (size_t)(kGroup * w) * kSlice + lane * 4;  // panel row of tile column 0
-  const float *E = Es + (size_t)(kGroup * w) * TW;
-#pragma unroll 2
-  for (int c = 0; c < TW; c += 4) {
-    float bv[4][4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) load4<T>(Bw + (size_t)(c + q) * kSlice, bv[q]);
-#pragma unroll
-    for (int r = 0; r < kGroup; ++r) {
-      const float4 v = *reinterpret_cast<const float4 *>(E + r * TW + c);
-      fma_vec<float, 4>(acc[r], v.x, bv[0]);
-      fma_vec<float, 4>(acc[r], v.y, bv[1]);
-      fma_vec<float, 4>(acc[r], v.z, bv[2]);
-      fma_vec<float, 4>(acc[r], v.w, bv[3]);
-    }
-  }
   const int col = col0 + lane * 4;
-  if (col < N) {
+  for (int k = 0; k < nb; ++k) {
+    const int rw = (g0 + k) * kCtaRows + kGroup * w;  // first C row of this warp
+    // the rest walk's C rows, kept packed until the end so that no FMA waits on them
+    Packed4<T> old[kGroup];
 #pragma unroll
     for (int r = 0; r < kGroup; ++r) {
-      const int row = i0 + kGroup * w + r;
-      if (row < M) {
-        T *cp = C + (int64_t)row * ldc + col;
-        float old[4];
-        load4_global<T>(cp, old);
+      if (rw + r < M && col < N) old[r].load_stream(C + (int64_t)(rw + r) * ldc + col);
+      else old[r].zero();
+    }
+    float acc[kGroup][4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc[r][k] += old[k];
-        store4<T>(cp, acc[r]);
+    for (int r = 0; r < kGroup; ++r) acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.f;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < NCH; ++j) bad |= !wait_phase(smem_addr(bar + (k + j) % NR), (uint32_t)(((k + j) / NR) & 1));
+    bad |= !wait_phase(smem_addr(bar + NR + (k & 1)), (uint32_t)((k >> 1) & 1));
+    if (__syncthreads_or(bad)) {
+      if (threadIdx.x == 0) {
+        atomicExch(&g_band_timeout, 1);
+        // give the copies still in flight a bounded chance to land before the block leaves
+        for (int c = max(0, issued_chunks - NR); c < issued_chunks; ++c)
+          wait_phase(smem_addr(bar + c % NR), (uint32_t)((c / NR) & 1));
+        for (int v = max(0, issued_vals - 2); v < issued_vals; ++v)
+          wait_phase(smem_addr(bar + NR + (v & 1)), (uint32_t)((v >> 1) & 1));
       }
+      return;
+    }
+    const int rb = (k % NR) * kChunk + kGroup * w;  // ring row of this warp's tile column 0
+    const float *E = vals + (size_t)(k & 1) * kCtaRows * TW + (size_t)(kGroup * w) * TW;
+#pragma unroll 2
+    for (int c = 0; c < TW; c += 4) {
+      int rr = rb + c;
+      if (rr >= RING_ROWS) rr -= RING_ROWS;  // four rows never straddle the wrap (all multiples of 4)
+      const T *bp = ring + (size_t)rr * kSlice + lane * 4;
+      float bv[4][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) load4<T>(bp + q * kSlice, bv[q]);
+      float4 v[kGroup];
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) v[r] = *reinterpret_cast<const float4 *>(E + r * TW + c);
+      // rows inner: consecutive FMAs update different accumulators
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) fma_vec<float, 4>(acc[r], v[r].x, bv[0]);
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) fma_vec<float, 4>(acc[r], v[r].y, bv[1]);
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) fma_vec<float, 4>(acc[r], v[r].z, bv[2]);
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) fma_vec<float, 4>(acc[r], v[r].w, bv[3]);
+    }
+    if (col < N) {
+#pragma unroll
+      for (int r = 0; r < kGroup; ++r) {
+        float o[4];
+        old[r].unpack(o);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[r][e] += o[e];
+        if (rw + r < M) store4<T>(C + (int64_t)(rw + r) * ldc + col, acc[r]);
+      }
+    }
+    __syncthreads();  // chunk k's slot and value slot k & 1 are free again
+    if (threadIdx.x == 0) {
+      if (k + NR < nchunks) issue_chunk(k + NR);
+      if (k + 2 < nb) issue_vals(k + 2);
     }
   }
 }
@@ -266,27 +338,38 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 template <class T, int TW>
 swift_status launch_tile(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
-                         cudaStream_t st) {
-  constexpr size_t smem = (size_t)panel_rows(TW) * kSlice * sizeof(T) + (size_t)kCtaRows * TW * 4 + 16;
-  constexpr int minb = smem * 2 <= 220 * 1024 ? 2 : 1;
+                         int sm_count, cudaStream_t st) {
+  constexpr int NR = (panel_rows(TW) + kChunk - 1) / kChunk + 1;
+  constexpr size_t smem = (size_t)NR * kChunk * kSlice * sizeof(T) + 2 * (size_t)kCtaRows * TW * 4 + (NR + 2) * 8;
+  // two blocks per SM where shared memory allows it and the 16-bit walk's registers fit (the FP32
+  // variant keeps its old-C rows in 32 more registers and would spill at 128)
+  constexpr int minb = sizeof(T) == 2 && smem * 2 + 2048 <= 227 * 1024 ? 2 : 1;
+  static_assert(smem <= 227 * 1024, "band tile kernel: shared memory above the per-block limit");
   auto k = band_tile_kernel<T, TW, minb>;
   SW_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const dim3 grid((unsigned)((M + kCtaRows - 1) / kCtaRows), (unsigned)((N + kSlice - 1) / kSlice));
-  k<<<grid, 256, smem, st>>>(map, tiles, M, N, W, static_cast<T *>(C), ldc);
+  int occ = 0;
+  SW_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem));
+  const int ngroups = (M + kCtaRows - 1) / kCtaRows, nslices = (N + kSlice - 1) / kSlice;
+  // one resident block per row range: contiguous ranges of 64-row groups, every SM filled
+  int ranges = std::max(1, std::min(ngroups, sm_count * std::max(occ, 1) / nslices));
+  const int per = (ngroups + ranges - 1) / ranges;
+  ranges = (ngroups + per - 1) / per;
+  k<<<dim3((unsigned)ranges, (unsigned)nslices), 256, smem, st>>>(map, tiles, M, N, W, ngroups, per,
+                                                                 static_cast<T *>(C), ldc);
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
 }
 
 template <class T>
 swift_status launch_tile_w(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
-                           cudaStream_t st) {
+                           int sm_count, cudaStream_t st) {
   switch (W) {
-    case 3: return launch_tile<T, tile_width(3)>(map, tiles, M, N, W, C, ldc, st);
-    case 7: return launch_tile<T, tile_width(7)>(map, tiles, M, N, W, C, ldc, st);
-    case 15: return launch_tile<T, tile_width(15)>(map, tiles, M, N, W, C, ldc, st);
-    case 31: return launch_tile<T, tile_width(31)>(map, tiles, M, N, W, C, ldc, st);
-    case 47: return launch_tile<T, tile_width(47)>(map, tiles, M, N, W, C, ldc, st);
-    case 63: return launch_tile<T, tile_width(63)>(map, tiles, M, N, W, C, ldc, st);
+    case 3: return launch_tile<T, tile_width(3)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 7: return launch_tile<T, tile_width(7)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 15: return launch_tile<T, tile_width(15)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 31: return launch_tile<T, tile_width(31)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 47: return launch_tile<T, tile_width(47)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 63: return launch_tile<T, tile_width(63)>(map, tiles, M, N, W, C, ldc, sm_count, st);
   }
   return SWIFT_ERR_UNSUPPORTED;
 }
@@ -414,11 +497,10 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
     return SWIFT_ERR_CUDA;
   }
   const size_t esz = d.dtype == SWIFT_F32 ? 4 : 2;
-  const int TW = tile_width(W);
   CUtensorMap map;
   cuuint64_t dims[2] = {(cuuint64_t)d.N, (cuuint64_t)std::max(p.K, 1)};
   cuuint64_t strides[1] = {(cuuint64_t)(d.ldb * (int64_t)esz)};
-  cuuint32_t box[2] = {(cuuint32_t)kSlice, (cuuint32_t)panel_rows(TW)};
+  cuuint32_t box[2] = {(cuuint32_t)kSlice, (cuuint32_t)kChunk};
   cuuint32_t es[2] = {1, 1};
   const CUtensorMapDataType dt = d.dtype == SWIFT_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : d.dtype == SWIFT_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
@@ -434,9 +516,9 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
   SW_TRY(run_merge(p, p.band_rest, d, o, st));
   const float *tiles = p.band_tiles.as<float>();
   switch (d.dtype) {
-    case SWIFT_F32: return launch_tile_w<float>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
-    case SWIFT_BF16: return launch_tile_w<__nv_bfloat16>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
-    case SWIFT_F16: return launch_tile_w<__half>(map, tiles, p.M, d.N, W, d.C, d.ldc, st);
+    case SWIFT_F32: return launch_tile_w<float>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
+    case SWIFT_BF16: return launch_tile_w<__nv_bfloat16>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
+    case SWIFT_F16: return launch_tile_w<__half>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
     default: return SWIFT_ERR_UNSUPPORTED;
   }
 }

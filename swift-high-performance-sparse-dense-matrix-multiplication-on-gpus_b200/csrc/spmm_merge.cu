@@ -446,8 +446,11 @@ __device__ __forceinline__ void flag_walk(const MergeArgs &a, int t, int sl, uns
 template <class T, class TA, class ACC, int VB, int SG, int MINB, bool FULL, bool SCALE = false>
 __global__ void __launch_bounds__(256, MINB) merge_flag_kernel(const MergeArgs a) {
   constexpr int G = 32 / SG;
-  __shared__ int2 stage_all[8 * G][32];
-  __shared__ ACC vstage_all[sizeof(TA) == 8 ? 8 * G : 1][32];
+  // one staging row per sub-warp, padded by one element: the sub-warps of a warp read their
+  // rows with broadcast loads in the same instruction, and unpadded 256-byte rows would put
+  // those reads on the same banks
+  __shared__ int2 stage_all[8 * G][33];
+  __shared__ ACC vstage_all[sizeof(TA) == 8 ? 8 * G : 1][33];
   const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
   const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
   const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G + sg;
@@ -721,8 +724,8 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
   constexpr int UNR = 4;
   constexpr int H = DODX ? SG / 2 : SG;
   constexpr bool F64 = sizeof(T) == 8;
-  __shared__ int2 stage_all[8 * G][32];
-  __shared__ T vstage_all[F64 ? 8 * G : 1][32];
+  __shared__ int2 stage_all[8 * G][33];  // padded as in merge_flag_kernel
+  __shared__ T vstage_all[F64 ? 8 * G : 1][33];
   const MergeArgs &a = ba.m;
   const int lane = threadIdx.x & 31, sg = lane / SG, sl = lane % SG;
   const unsigned sgmask = SG == 32 ? 0xffffffffu : (((1u << SG) - 1u) << (sg * SG));
@@ -900,7 +903,7 @@ __global__ void __launch_bounds__(256, 4) merge_batch_kernel(const MergeArgs *__
                                                              const int *__restrict__ shape,
                                                              const int64_t *__restrict__ item_off,
                                                              int count) {
-  __shared__ int2 stage_all[8 * 4][32];
+  __shared__ int2 stage_all[8 * 4][33];  // padded as in merge_flag_kernel
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t total = __ldg(item_off + count);
   const int64_t nw = (int64_t)gridDim.x * 8;
