@@ -51,6 +51,8 @@ WORKLOADS = {
     "rmat19band_n128_bf16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="bf16"),
     "rmat19band_n128_f16": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f16"),
     "rmat19band_n128_f32": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f32"),
+    # half-size banded case for full ncu captures of the band engine (B and C exceed L2)
+    "rmat18band_n128_f32": dict(kind="rmatband", scale=18, edges=8 << 20, N=128, dtype="f32"),
     # precision ratios (FP32 vs BF16 vs FP16 B/C on one FP32-valued matrix)
     "precision_rmat19band_n128": dict(kind="precision", rk="rmatband", scale=19, edges=16 << 20, N=128),
     # differentiation: GNN layer on a symmetric-normalised R-MAT graph, fused vs plain
@@ -473,6 +475,27 @@ def run_precision(args):
                      "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / peak, "clocks": clk}
     del ref
     f32b, bfb = res["f32"]["algorithmic_bytes"], res["bf16"]["algorithmic_bytes"]
+    # the band engine's own format: dense 8-row tiles (values only) + the rest as CSR
+    hist, bw = plan.band_profile()
+    band = None
+    if bw >= 0:
+        tw = (8 + 2 * bw + 3) // 4 * 4
+        rows = np.repeat(np.arange(M, dtype=np.int64), np.diff(rp.astype(np.int64)))
+        c0 = (rows & ~7) - bw
+        cols = ci.astype(np.int64)
+        rest_nnz = int(np.count_nonzero((cols < c0) | (cols >= c0 + tw)))
+        del rows, c0, cols
+        tile_bytes = ((M + 63) // 64) * 64 * tw * 4
+        band = {"half_width": bw, "tile_width": tw, "tile_bytes": tile_bytes, "rest_nnz": rest_nnz,
+                "in_tiles_nnz": nnz - rest_nnz}
+        for name in ("f32", "bf16", "f16"):
+            esz = 4 if name == "f32" else 2
+            b = tile_bytes + rest_nnz * 8 + (K + M) * N * esz
+            band[f"format_bytes_{name}"] = b
+            if res[name]["engine"] == "band":
+                res[name]["algorithmic_bytes_band_format"] = b
+                res[name]["hbm_frac_band_format"] = b / (res[name]["ms"] / 1e3) / 1e9 / peak
+        band["byte_ceiling_16bit_vs_f32"] = band["format_bytes_f32"] / band["format_bytes_bf16"]
     cpu = None
     if not args.no_cpu_baseline:
         try:  # the reference has no 16-bit path: its FP32 Swift_cpu on the same matrix and B
@@ -492,7 +515,10 @@ def run_precision(args):
         "ratio_bf16_vs_f32": res["f32"]["ms"] / res["bf16"]["ms"],
         "ratio_f16_vs_f32": res["f32"]["ms"] / res["f16"]["ms"],
         "byte_model_ceiling_16bit_vs_f32": f32b / bfb,
-        "roofline": roofline_line(bfb, res["bf16"]["ms"], args.workload, "merge_flag_kernel"),
+        "band_format": band,
+        "roofline": roofline_line(res["bf16"].get("algorithmic_bytes_band_format", bfb), res["bf16"]["ms"],
+                                  args.workload, "band_tile_kernel + merge_flag_kernel" if res["bf16"]["engine"] == "band"
+                                  else "merge_flag_kernel"),
         "products": res,
         "gpu_launches": args.steps,
         "clocks": merge_clocks([r["clocks"] for r in res.values()]),
@@ -838,6 +864,8 @@ def run_ours(args):
         U, unr, vb, kern = (int(x) for x in args.rowwise_params.split(","))
         plan.set_rowwise_params(U, unr, vb, kern)
         engine, tune_ms, tune_wall_ms = "rowwise", None, 0.0
+    elif args.engine != "auto":  # a pinned engine (profiling): no autotuning
+        engine, tune_ms, tune_wall_ms = args.engine, None, 0.0
     else:
         torch.cuda.synchronize()
         tw0 = time.perf_counter()
@@ -847,8 +875,9 @@ def run_ours(args):
     rw_params = plan.rowwise_params(N, B.dtype) if engine == "rowwise" else None
     st = plan.stats()
     stream = torch.cuda.current_stream()
+    run_engine = args.engine if not args.rowwise_params else "auto"
     for _ in range(args.warmup):
-        plan.spmm(B, C)
+        plan.spmm(B, C, engine=run_engine)
     gpu_idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[local] if os.environ.get("CUDA_VISIBLE_DEVICES") else local
     sampler = ClockSampler(gpu_idx)
     if dist:
@@ -859,7 +888,7 @@ def run_ours(args):
     w0 = time.time()
     e0.record(stream)
     for _ in range(args.steps):
-        plan.spmm(B, C)
+        plan.spmm(B, C, engine=run_engine)
     e1.record(stream)
     torch.cuda.synchronize()
     w1 = time.time()
@@ -895,7 +924,19 @@ def run_ours(args):
         t_ms = e0.elapsed_time(e1) / n_t
         tiled = {"gflops": flops / (t_ms / 1e3) / 1e9, "ms_per_step": t_ms,
                  "hbm_frac_of_measured": alg_bytes / (t_ms / 1e3) / 1e9 / peak}
-        plan.spmm(B, C)
+        plan.spmm(B, C, engine=run_engine)
+
+    # the gather ceiling of row-ordered products on this matrix: a kernel that only gathers the
+    # B rows of A's column stream (swift_gather_bound), and the same with L1-resident rows
+    gather = None
+    if B.dtype == torch.float32 and N in (32, 64, 128) and K >= 256:
+        g_ms, g_l1, _ = plan.gather_bound(B, reps=10)
+        gbytes = nnz * N * 4
+        gather = {"what": "B rows gathered along A's column stream only (no values, no C)",
+                  "gather_bytes_per_launch": gbytes, "ms_column_stream": g_ms, "ms_l1_resident": g_l1,
+                  "tb_s_column_stream": gbytes / (g_ms / 1e3) / 1e12, "tb_s_l1_resident": gbytes / (g_l1 / 1e3) / 1e12,
+                  "product_time_over_gather_time": ms_step / g_ms}
+        plan.spmm(B, C, engine=run_engine)
 
     # context only: the vendor library's CSR SpMM (torch.sparse -> cuSPARSE) on the same inputs
     library = None
@@ -934,7 +975,7 @@ def run_ours(args):
             s_c.wait_event(ev_in[j])
             if i >= 2:
                 s_c.wait_event(ev_out[j])  # Cd[j] free once it was copied out
-            plan.spmm(Bd[j], Cd[j], stream=s_c)
+            plan.spmm(Bd[j], Cd[j], engine=run_engine, stream=s_c)
             ev_c[j].record(s_c)
             with torch.cuda.stream(s_out):
                 s_out.wait_event(ev_c[j])
@@ -1020,6 +1061,7 @@ def run_ours(args):
         "clocks": clocks,
         "cpu_baseline": cpu,
         "tiled_engine": tiled,
+        "gather_bound": gather,
         "library_context": library,
     }
     print(json.dumps(out), flush=True)
@@ -1259,6 +1301,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", type=float, default=150.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--engine", choices=["auto", "rowwise", "tiled", "tiled_grouped", "band"], default="auto",
+                    help="single-product workloads: run this engine instead of the autotuned choice (profiling)")
     ap.add_argument("--rowwise-params", help="task_size,loads_in_flight,vector_bytes,kernel: run the row "
                                              "engine with these instead of autotuning (e.g. for a profile)")
     ap.add_argument("--mtx", help="MatrixMarket coordinate file: run the product on this matrix instead "

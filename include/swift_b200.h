@@ -321,6 +321,17 @@ swift_status swift_spmm_noalloc(const swift_plan *plan, int N, swift_dtype dtype
 swift_status swift_plan_band_profile(swift_plan *plan, long long *hist, int *half_width,
                                      swift_stream_t stream);
 
+/* Measurement: the gather ceiling of the row-ordered engines on this plan's A.  Times (CUDA
+ * events on `stream`, `reps` launches after two warm-up launches) a kernel that only gathers B
+ * rows along A's column stream -- the row walk's 16-byte vectors and sub-warp widths, four
+ * loads in flight per lane, no values, no row bookkeeping, no C -- and the same kernel with
+ * every column index folded into rows 0..255 (rows resident in L1).  ms_stream and ms_l1 are
+ * per launch; checksum (may be NULL) is the sum of every gathered element of the first launch
+ * kind, for checking.  Row-major FP32 B (K x N), N in {32, 64, 128}, B 16-byte aligned,
+ * ldb % 4 == 0, K >= 256.  Synchronises `stream`.  No counterpart in the reference. */
+swift_status swift_gather_bound(const swift_plan *plan, int N, const float *B, int64_t ldb, int reps,
+                                swift_stream_t stream, double *ms_stream, double *ms_l1, double *checksum);
+
 /* Whether a BAND product's block gave up waiting for its TMA copies (a bounded wait of about
  * two seconds; the block then leaves its C rows without the tiles' part): *flag = 1 if any did
  * since the last reset.  Synchronous; reset != 0 clears the flag.  No counterpart in the

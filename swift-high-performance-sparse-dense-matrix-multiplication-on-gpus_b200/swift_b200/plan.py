@@ -353,6 +353,17 @@ class Plan:
         return {capi.ENGINE_TILED: "tiled", capi.ENGINE_ROWWISE: "rowwise",
                 capi.ENGINE_TILED_GROUPED: "tiled_grouped", capi.ENGINE_BAND: "band"}[eng.value], ms.value
 
+    def gather_bound(self, B, reps=10, stream=None):
+        """(ms_stream, ms_l1, checksum): the time per launch of a kernel that only gathers B rows
+        along A's column stream, the same with every row L1-resident, and the sum of the gathered
+        elements (swift_gather_bound; FP32 row-major B, N in 32/64/128)."""
+        N = int(B.shape[1])
+        _dense(B, self.K, N, "B")
+        a, b, c = C.c_double(0), C.c_double(0), C.c_double(0)
+        capi.check(capi.lib().swift_gather_bound(self._h, N, B.data_ptr(), _ld(B, 0), reps, _stream_ptr(stream),
+                                                 C.byref(a), C.byref(b), C.byref(c)), "swift_gather_bound")
+        return a.value, b.value, c.value
+
     def band_profile(self, stream=None):
         """(hist, half_width): nonzeros per |col - row| for 0..128 (measured on the GPU) and the
         band engine's half-width (-1 when no width pays)."""
