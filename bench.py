@@ -828,6 +828,38 @@ def run_batch(args):
     batch.close()
 
 
+def run_block_histogram(args):
+    """Block-density histograms of the workload's matrix, measured on the GPU: for each block
+    shape, occupied blocks and their nonzeros per fill bin (bin k: fill in (2^-(k+1), 2^-k],
+    the last bin sparser), in A's own column order and in the plan's sorted column order."""
+    import torch
+
+    from swift_b200 import Plan
+    wl = dict(WORKLOADS[args.workload])
+    if wl["kind"] == "precision":
+        wl = dict(wl, kind=wl["rk"], dtype="f32")
+    if wl["kind"] not in ("rmat", "rmatband", "poisson", "mtx"):
+        raise SystemExit(f"--block-histogram: workload kind {wl['kind']} has no single matrix")
+    M, K, rp, ci, val, _ = make_inputs(wl, "cuda")
+    plan = Plan.from_csr(torch.from_numpy(rp).cuda(), torch.from_numpy(ci).cuda(), val, (M, K))
+    nbins = 8
+    out = {"workload": args.workload, "rows": M, "cols": K, "nnz": int(rp[-1]),
+           "bins": [f"({2.0 ** -(k + 1):g}, {2.0 ** -k:g}]" for k in range(nbins - 1)] + [f"<= {2.0 ** -(nbins - 1):g}"],
+           "histograms": []}
+    for shape in args.block_histogram.split(","):
+        bh, bw = (int(x) for x in shape.lower().split("x"))
+        for sorted_cols in (False, True):
+            blocks, nnz = plan.block_histogram(bh, bw, sorted_columns=sorted_cols, nbins=nbins)
+            out["histograms"].append({"block": f"{bh}x{bw}", "columns": "sorted" if sorted_cols else "original",
+                                      "blocks": blocks.tolist(), "nnz": nnz.tolist(),
+                                      "nnz_share": (nnz / max(1, nnz.sum())).round(4).tolist()})
+    hist, bw_ = plan.band_profile()
+    out["band_half_width"] = bw_
+    out["nnz_within_distance"] = {str(d): int(hist[: d + 1].sum()) for d in (0, 3, 7, 15, 31, 63, 128)}
+    print(json.dumps(out), flush=True)
+    plan.close()
+
+
 def run_ours(args):
     import torch
 
@@ -1305,6 +1337,9 @@ def main():
                     help="single-product workloads: run this engine instead of the autotuned choice (profiling)")
     ap.add_argument("--rowwise-params", help="task_size,loads_in_flight,vector_bytes,kernel: run the row "
                                              "engine with these instead of autotuning (e.g. for a profile)")
+    ap.add_argument("--block-histogram", metavar="BHxBW[,BHxBW...]",
+                    help="instead of timing: print the block-density histograms of the workload's matrix "
+                         "(swift_plan_block_histogram, A's and the sorted column order) as one JSON line")
     ap.add_argument("--mtx", help="MatrixMarket coordinate file: run the product on this matrix instead "
                                   "of a synthetic workload")
     ap.add_argument("--n", type=int, default=128, help="dense columns with --mtx")
@@ -1316,7 +1351,9 @@ def main():
         args.workload = name
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    if args.impl == "reference":
+    if args.block_histogram:
+        run_block_histogram(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-gpu":
         run_reference_gpu(args)

@@ -321,6 +321,17 @@ swift_status swift_spmm_noalloc(const swift_plan *plan, int N, swift_dtype dtype
 swift_status swift_plan_band_profile(swift_plan *plan, long long *hist, int *half_width,
                                      swift_stream_t stream);
 
+/* Block-density histogram of A, measured on the GPU: blocks of bh consecutive rows x bw
+ * consecutive columns, columns in A's own order (order 0) or the plan's sorted column order
+ * (order 1).  For each block holding a nonzero, its fill f = nonzeros / (bh * bw) lands in bin
+ * k when 2^-(k+1) < f <= 2^-k (k = 0 .. nbins - 2) and in bin nbins - 1 when sparser;
+ * blocks[k] counts those blocks and nnz[k] their nonzeros (both arrays nbins long, host
+ * memory, 1 <= nbins <= 64).  Synchronises `stream`; temporary device memory of about 20 bytes
+ * per nonzero.  The measurement behind a dense-tile path (the BAND engine, tensor cores): it
+ * pays only where blocks are dense.  No counterpart in the reference. */
+swift_status swift_plan_block_histogram(swift_plan *plan, int bh, int bw, int order, int nbins,
+                                        long long *blocks, long long *nnz, swift_stream_t stream);
+
 /* Measurement: the gather ceiling of the row-ordered engines on this plan's A.  Times (CUDA
  * events on `stream`, `reps` launches after two warm-up launches) a kernel that only gathers B
  * rows along A's column stream -- the row walk's 16-byte vectors and sub-warp widths, four

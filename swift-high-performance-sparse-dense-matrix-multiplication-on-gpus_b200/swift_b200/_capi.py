@@ -128,6 +128,7 @@ _SIGS = [
     ("swift_plan_is_symmetric", C.c_int, [_P, C.POINTER(C.c_int), _P]),
     ("swift_plan_band_profile", C.c_int, [_P, _P, C.POINTER(C.c_int), _P]),
     ("swift_band_timeout_flag", C.c_int, [C.POINTER(C.c_int), C.c_int]),
+    ("swift_plan_block_histogram", C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
     ("swift_gather_bound", C.c_int, [_P, C.c_int, _P, _I64, C.c_int, _P, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("swift_plan_set_symmetry", C.c_int, [_P, C.c_int]),

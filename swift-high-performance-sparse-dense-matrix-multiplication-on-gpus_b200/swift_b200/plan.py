@@ -364,6 +364,16 @@ class Plan:
                                                  C.byref(a), C.byref(b), C.byref(c)), "swift_gather_bound")
         return a.value, b.value, c.value
 
+    def block_histogram(self, bh, bw, sorted_columns=False, nbins=8, stream=None):
+        """(blocks, nnz): occupied bh x bw blocks of A binned by fill f, bin k = (2^-(k+1), 2^-k]
+        (the last bin: sparser), and their nonzeros (swift_plan_block_histogram)."""
+        blocks = np.zeros(nbins, np.int64)
+        nnz = np.zeros(nbins, np.int64)
+        capi.check(capi.lib().swift_plan_block_histogram(self._h, bh, bw, int(bool(sorted_columns)), nbins,
+                                                         blocks.ctypes.data, nnz.ctypes.data, _stream_ptr(stream)),
+                   "swift_plan_block_histogram")
+        return blocks, nnz
+
     def band_profile(self, stream=None):
         """(hist, half_width): nonzeros per |col - row| for 0..128 (measured on the GPU) and the
         band engine's half-width (-1 when no width pays)."""
