@@ -397,10 +397,15 @@ swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream);
 /* Captures swift_batch_run into a CUDA graph on the first call (on a private stream) and
  * replays it on `stream`. */
 swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream);
-/* Times the batch with tasks of 256, 512 and 1024 merged positions and keeps the fastest
- * (operands must be set; each C_i is overwritten with its product). */
+/* Chooses the merge-path task size (merged positions per sub-warp task) per member class --
+ * N <= 32, N <= 64, wider -- by timing whole batch launches: the best of 128, 256, 512 and 1024
+ * for every class, then each class on its own against the others' current sizes (operands
+ * must be set; each C_i is overwritten with its product).  best_ms = the chosen launch's time,
+ * best_task_size = the widest class's size. */
 swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, double *best_ms,
                                   int *best_task_size);
+/* The task sizes in use for the three member classes (N <= 32, N <= 64, wider). */
+swift_status swift_batch_get_task_sizes(const swift_batch *batch, int *sizes);
 
 /* ------------------------------------------------------------------ MatrixMarket input */
 /* Reads a MatrixMarket coordinate file into host CSR as the reference's reader does

@@ -19,7 +19,9 @@ struct swift_batch {
   };
   int device = 0;
   int count = 0;
-  int U = 512;
+  // merge-path task size per member class: N <= 32, N <= 64, wider (each class has its own
+  // best grain: narrow rows favour small tasks, wide rows large ones)
+  int U[3] = {512, 512, 512};
   int grid = 0;
   std::vector<swift_plan *> plans;
   std::vector<std::unique_ptr<swift::RowLayout>> layouts;
@@ -45,6 +47,8 @@ namespace {
 
 cudaStream_t to_stream(swift_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+int member_class(int N) { return N <= 32 ? 0 : (N <= 64 ? 1 : 2); }
+
 swift_status on_device(const swift_batch *b) {
   int dev = -1;
   SW_CHECK_CUDA(cudaGetDevice(&dev));
@@ -62,7 +66,8 @@ swift_status build_table(swift_batch *b, cudaStream_t st) {
   for (int i = 0; i < b->count; ++i) {
     b->h_off[i] = off;
     int64_t items = 0;
-    SW_TRY(merge_batch_member(b->plans[i]->p, *b->layouts[i], b->U, b->ops.N[i], b->ops.B[i], b->ops.ldb[i],
+    SW_TRY(merge_batch_member(b->plans[i]->p, *b->layouts[i], b->U[member_class(b->ops.N[i])], b->ops.N[i],
+                              b->ops.B[i], b->ops.ldb[i],
                               b->ops.C[i], b->ops.ldc[i], b->h_args.data() + asz * i, &b->h_shape[i], &items,
                               st));
     off += items;
@@ -195,31 +200,60 @@ swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, dou
   cudaEvent_t e0, e1;
   SW_CHECK_CUDA(cudaEventCreate(&e0));
   SW_CHECK_CUDA(cudaEventCreate(&e1));
-  double best = 1e300;
-  int bestU = batch->U;
-  swift_status rc = SWIFT_OK;
-  for (int U : {256, 512, 1024}) {
-    batch->U = U;
+  // ms per launch with the task sizes in `U`, or < 0 on failure
+  auto time_sizes = [&](const int (&U)[3], swift_status &rc) -> double {
+    for (int c = 0; c < 3; ++c) batch->U[c] = U[c];
     rc = build_table(batch, st);
     for (int w = 0; w < 2 && rc == SWIFT_OK; ++w) rc = launch(batch, st);
-    if (rc != SWIFT_OK) break;
+    if (rc != SWIFT_OK) return -1.0;
     const int reps = 5;
     cudaEventRecord(e0, st);
     for (int r = 0; r < reps && rc == SWIFT_OK; ++r) rc = launch(batch, st);
     cudaEventRecord(e1, st);
-    if (rc != SWIFT_OK) break;
+    if (rc != SWIFT_OK) return -1.0;
     cudaEventSynchronize(e1);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    if (ms / reps < best) { best = ms / reps; bestU = U; }
+    return ms / reps;
+  };
+  // coordinate descent: the best size for all classes, then each class on its own
+  const int cands[] = {128, 256, 512, 1024};
+  bool present[3] = {false, false, false};
+  for (int i = 0; i < batch->count; ++i) present[member_class(batch->ops.N[i])] = true;
+  double best = 1e300;
+  int bestU[3] = {batch->U[0], batch->U[1], batch->U[2]};
+  swift_status rc = SWIFT_OK;
+  for (int u : cands) {
+    const int U[3] = {u, u, u};
+    const double ms = time_sizes(U, rc);
+    if (rc != SWIFT_OK) break;
+    if (ms < best) { best = ms; bestU[0] = bestU[1] = bestU[2] = u; }
+  }
+  for (int c = 0; c < 3 && rc == SWIFT_OK; ++c) {
+    if (!present[c]) continue;
+    const int keep = bestU[c];
+    for (int u : cands) {
+      if (u == keep) continue;
+      int U[3] = {bestU[0], bestU[1], bestU[2]};
+      U[c] = u;
+      const double ms = time_sizes(U, rc);
+      if (rc != SWIFT_OK) break;
+      if (ms < best) { best = ms; bestU[c] = u; }
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  batch->U = bestU;
+  for (int c = 0; c < 3; ++c) batch->U[c] = bestU[c];
   if (rc == SWIFT_OK) rc = build_table(batch, st);
   if (rc != SWIFT_OK) return rc;
   if (best_ms) *best_ms = best;
-  if (best_task_size) *best_task_size = bestU;
+  if (best_task_size) *best_task_size = bestU[2];
+  return SWIFT_OK;
+}
+
+swift_status swift_batch_get_task_sizes(const swift_batch *batch, int *sizes) {
+  if (!batch || !sizes) return SWIFT_ERR_INVALID_ARG;
+  for (int c = 0; c < 3; ++c) sizes[c] = batch->U[c];
   return SWIFT_OK;
 }
 

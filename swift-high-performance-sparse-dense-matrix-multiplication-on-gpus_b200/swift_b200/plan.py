@@ -425,11 +425,18 @@ class Batch:
         capi.check(capi.lib().swift_batch_run_graph(self._h, _stream_ptr(stream)), "swift_batch_run_graph")
 
     def autotune(self, stream=None):
-        """Chooses the task size over the whole batch; returns (task_size, ms per run)."""
+        """Chooses the task size per member class (N <= 32, N <= 64, wider); returns (the widest
+        class's task size, ms per run)."""
         ms, U = C.c_double(0), C.c_int(0)
         capi.check(capi.lib().swift_batch_autotune(self._h, _stream_ptr(stream), C.byref(ms), C.byref(U)),
                    "swift_batch_autotune")
         return U.value, ms.value
+
+    def task_sizes(self):
+        """The task sizes in use for the member classes N <= 32, N <= 64 and wider."""
+        out = (C.c_int * 3)()
+        capi.check(capi.lib().swift_batch_get_task_sizes(self._h, out), "swift_batch_get_task_sizes")
+        return list(out)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -82,7 +82,9 @@ def test_batch_autotune_keeps_results():
     b = Batch(plans)
     b.set_operands(Bs, Cs)
     U, ms_run = b.autotune()
-    assert U in (256, 512, 1024) and ms_run > 0
+    sizes = b.task_sizes()
+    assert U in (128, 256, 512, 1024) and ms_run > 0
+    assert sizes[2] == U and all(s in (128, 256, 512, 1024) for s in sizes)
     for c in Cs:
         c.fill_(float("nan"))
     b.run()
