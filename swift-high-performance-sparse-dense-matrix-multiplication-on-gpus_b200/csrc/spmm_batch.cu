@@ -4,6 +4,7 @@
 // shares task arrays, split counters or scratch with the plan's own products); the launch
 // records of all members live in one device table that the persistent kernel reads, so
 // setting new operands only rewrites the table and a captured CUDA graph stays valid.
+#include <algorithm>
 #include <memory>
 #include <vector>
 
@@ -24,6 +25,11 @@ struct swift_batch {
   int U[3] = {512, 512, 512};
   int grid = 0;
   std::vector<swift_plan *> plans;
+  // the order the persistent grid walks the members in: flattest column distribution first
+  // (share of nonzeros in the top 1 % of columns, ascending; stable).  Members with a flat
+  // distribution gather across their whole B; walking them before the skewed ones measured
+  // fastest (batch512: 8.48 ms against 9.7-10.2 ms for shuffled or skewed-first orders).
+  std::vector<int> order;
   std::vector<std::unique_ptr<swift::RowLayout>> layouts;
   std::vector<unsigned char> h_args;
   std::vector<int> h_shape;
@@ -63,12 +69,13 @@ swift_status on_device(const swift_batch *b) {
 swift_status build_table(swift_batch *b, cudaStream_t st) {
   const size_t asz = merge_args_size();
   int64_t off = 0;
-  for (int i = 0; i < b->count; ++i) {
-    b->h_off[i] = off;
+  for (int k = 0; k < b->count; ++k) {
+    const int i = b->order[k];  // table slot k holds member i
+    b->h_off[k] = off;
     int64_t items = 0;
     SW_TRY(merge_batch_member(b->plans[i]->p, *b->layouts[i], b->U[member_class(b->ops.N[i])], b->ops.N[i],
                               b->ops.B[i], b->ops.ldb[i],
-                              b->ops.C[i], b->ops.ldc[i], b->h_args.data() + asz * i, &b->h_shape[i], &items,
+                              b->ops.C[i], b->ops.ldc[i], b->h_args.data() + asz * k, &b->h_shape[k], &items,
                               st));
     off += items;
   }
@@ -127,6 +134,23 @@ swift_status swift_batch_create(swift_plan *const *plans, int count, swift_strea
   b->device = dev;
   b->count = count;
   b->plans.assign(plans, plans + count);
+  {
+    std::vector<double> skew((size_t)count, 0.0);
+    for (int i = 0; i < count; ++i) {
+      const Plan &p = plans[i]->p;
+      const int t = std::max(1, p.K / 100);
+      if (p.K == 0 || p.nnz == 0) continue;
+      std::vector<int> tail((size_t)t);
+      SW_CHECK_CUDA(cudaMemcpy(tail.data(), p.sortnnz.as<int>() + (p.K - t), sizeof(int) * (size_t)t,
+                               cudaMemcpyDeviceToHost));
+      int64_t sum = 0;
+      for (int c : tail) sum += c;
+      skew[(size_t)i] = (double)sum / (double)p.nnz;
+    }
+    b->order.resize((size_t)count);
+    for (int i = 0; i < count; ++i) b->order[(size_t)i] = i;
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return skew[(size_t)x] < skew[(size_t)y]; });
+  }
   for (int i = 0; i < count; ++i) b->layouts.emplace_back(new RowLayout());
   b->h_args.assign(merge_args_size() * (size_t)std::max(count, 1), 0);
   b->h_shape.assign((size_t)std::max(count, 1), 0);

@@ -190,6 +190,24 @@ def test_band_autotune_picks_band_and_auto_runs_it():
     pl.close()
 
 
+def test_band_empty_and_tiny_matrices():
+    """No nonzeros at all (every C row written as zeros), and fewer rows than one 64-row group."""
+    B = torch.from_numpy(gen.dense_uniform(300, 128, seed=21)).cuda()
+    rp = np.zeros(501, np.int32)
+    pl = Plan.from_csr(rp, np.zeros(0, np.int32), np.zeros(0, np.float32), (500, 300))
+    C = torch.full((500, 128), 5.0, device="cuda")
+    pl.spmm(B, C_out=C, engine="band")
+    assert torch.count_nonzero(C).item() == 0
+    pl.close()
+    rp, ci = band_pattern(5, 300, 3)
+    val = gen.uniform_values(len(ci), seed=22)
+    pl = Plan.from_csr(rp, ci, val, (5, 300))
+    C = pl.spmm(B, engine="band")
+    ref = oracle.pipeline(5, 300, rp, ci, val, B.cpu().numpy())["C"]
+    assert relerr(C.cpu().numpy(), ref) <= 1e-5
+    pl.close()
+
+
 def test_band_no_timeouts():
     from swift_b200 import _capi as capi
     import ctypes as C
