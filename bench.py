@@ -443,6 +443,7 @@ def run_precision(args):
         B = B32.to(dt)
         C = torch.empty((M, N), dtype=dt, device="cuda")
         eng, _ = plan.autotune(B, C)
+        rw = plan.rowwise_params(N, dt) if eng in ("rowwise", "band") else None
         ms, clk = _timed_clocked(lambda: plan.spmm(B, C), args.steps, args.warmup, local)
         plan.spmm(B, C)
         err = (C.double() - ref).abs().max().item() / refmax
@@ -454,7 +455,7 @@ def run_precision(args):
             del ref_q
         bytes_ = nnz * 8 + (K + M) * N * B.element_size()
         res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": eng,
-                     "err_vs_fp64": err, "err_vs_fp64_on_rounded_B": err_in,
+                     "row_engine_params": rw, "err_vs_fp64": err, "err_vs_fp64_on_rounded_B": err_in,
                      "algorithmic_bytes": bytes_, "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / peak, "clocks": clk}
     # 16-bit B and C with per-row power-of-two scales (swift_spmm_scaled): B rows stored as
     # B / b_scale with each row's maximum in [2^14, 2^15); error of c_scale * C against FP64
@@ -473,6 +474,11 @@ def run_precision(args):
         res[name] = {"ms": ms, "gflops": 2.0 * nnz * N / (ms / 1e3) / 1e9, "engine": "rowwise",
                      "err_vs_fp64": err, "algorithmic_bytes": bytes_,
                      "hbm_frac": bytes_ / (ms / 1e3) / 1e9 / peak, "clocks": clk}
+    # the plain FP32 path: the row walk over all of A, whatever the autotuner picked above
+    B = B32
+    C = torch.empty((M, N), dtype=torch.float32, device="cuda")
+    ms_rw, clk_rw = _timed_clocked(lambda: plan.spmm(B, C, engine="rowwise"), args.steps, args.warmup, local)
+    plain_f32 = {"ms": ms_rw, "gflops": 2.0 * nnz * N / (ms_rw / 1e3) / 1e9, "engine": "rowwise", "clocks": clk_rw}
     del ref
     f32b, bfb = res["f32"]["algorithmic_bytes"], res["bf16"]["algorithmic_bytes"]
     # the band engine's own format: dense 8-row tiles (values only) + the rest as CSR
@@ -514,6 +520,11 @@ def run_precision(args):
                    "description": describe(args.workload, dict(wl, kind="rmatband", dtype="bf16/f16/f32"), nnz)},
         "ratio_bf16_vs_f32": res["f32"]["ms"] / res["bf16"]["ms"],
         "ratio_f16_vs_f32": res["f32"]["ms"] / res["f16"]["ms"],
+        "plain_f32_path": plain_f32,
+        "ratio_bf16_vs_plain_f32_path": plain_f32["ms"] / res["bf16"]["ms"],
+        "ratio_f16_vs_plain_f32_path": plain_f32["ms"] / res["f16"]["ms"],
+        "ratios_note": ("ratio_*_vs_f32: against the autotuned FP32 product (the band engine on this matrix); "
+                        "ratio_*_vs_plain_f32_path: against the FP32 row walk over all of A"),
         "byte_model_ceiling_16bit_vs_f32": f32b / bfb,
         "band_format": band,
         "roofline": roofline_line(res["bf16"].get("algorithmic_bytes_band_format", bfb), res["bf16"]["ms"],
@@ -521,7 +532,7 @@ def run_precision(args):
                                   else "merge_flag_kernel"),
         "products": res,
         "gpu_launches": args.steps,
-        "clocks": merge_clocks([r["clocks"] for r in res.values()]),
+        "clocks": merge_clocks([r["clocks"] for r in res.values()] + [clk_rw]),
         "clocks_headline": res["bf16"]["clocks"],
         "cpu_baseline": cpu,
     }
@@ -893,10 +904,10 @@ def run_ours(args):
     d_ci = torch.from_numpy(ci).cuda()
     plan = Plan.from_csr(d_rp, d_ci, val, (M, K))
     C = torch.empty((M, N), dtype=B.dtype, device="cuda")
-    if args.rowwise_params:
+    if args.rowwise_params:  # with --engine band they set the band engine's rest walk
         U, unr, vb, kern = (int(x) for x in args.rowwise_params.split(","))
         plan.set_rowwise_params(U, unr, vb, kern)
-        engine, tune_ms, tune_wall_ms = "rowwise", None, 0.0
+        engine, tune_ms, tune_wall_ms = ("band" if args.engine == "band" else "rowwise"), None, 0.0
     elif args.engine != "auto":  # a pinned engine (profiling): no autotuning
         engine, tune_ms, tune_wall_ms = args.engine, None, 0.0
     else:
@@ -908,7 +919,7 @@ def run_ours(args):
     rw_params = plan.rowwise_params(N, B.dtype) if engine == "rowwise" else None
     st = plan.stats()
     stream = torch.cuda.current_stream()
-    run_engine = args.engine if not args.rowwise_params else "auto"
+    run_engine = args.engine if (not args.rowwise_params or args.engine == "band") else "auto"
     for _ in range(args.warmup):
         plan.spmm(B, C, engine=run_engine)
     gpu_idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[local] if os.environ.get("CUDA_VISIBLE_DEVICES") else local

@@ -536,7 +536,18 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
       std::lock_guard<std::mutex> g(p.mu);
       if (band_profile(p, st) == SWIFT_OK) w = p.band_w;
     }
-    if (w >= 0) cands.push_back({SWIFT_ENGINE_BAND, MergeOpts{}});
+    if (w >= 0) {
+      // the band engine's rest walk: task size x vector width (the tiles take no parameters)
+      for (int U : {256, 512, 1024})
+        for (int vb : {16, 32}) {
+          MergeOpts mo;
+          mo.U = U;
+          mo.unroll = 4;
+          mo.vbytes = vb;
+          mo.kernel = 2;
+          cands.push_back({SWIFT_ENGINE_BAND, mo});
+        }
+    }
   }
   if (p.has_csr) {
     // task size (the work-balance grain) x (loads in flight, vector bytes, kernel variant)
@@ -592,7 +603,7 @@ swift_status swift_plan_autotune(swift_plan *plan, int N, swift_dtype dtype, con
   {
     std::lock_guard<std::mutex> g(p.mu);
     p.tuned[{N, (int)dtype}] = win.eng;
-    if (win.eng == SWIFT_ENGINE_ROWWISE) p.tuned_merge[{N, (int)dtype}] = win.mo;
+    if (win.eng == SWIFT_ENGINE_ROWWISE || win.eng == SWIFT_ENGINE_BAND) p.tuned_merge[{N, (int)dtype}] = win.mo;
   }
   if (best_ms) *best_ms = best;
   if (best_engine) *best_engine = win.eng;
