@@ -857,9 +857,14 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
         }
       }
       if (DODA) {
-        const T r = reduce4<T, SG>(part[0], part[1], part[2], part[3], sl, sgmask);
-        const int idx = ((sl & (SG / 2)) ? 2 : 0) + ((sl & (SG / 4)) ? 1 : 0);
-        if ((sl & (SG / 4 - 1)) == 0 && k + idx < m) dA[q0 + k + idx] = r;
+        // with DODX only the X half holds partial dot products: reduce over it alone when it has
+        // the four lanes the four-value reduction needs
+        constexpr bool HALF = DODX && H >= 4;
+        constexpr int RW = HALF ? H : SG;
+        const int rl = HALF ? lsl : sl;
+        const T r = reduce4<T, RW>(part[0], part[1], part[2], part[3], rl, sgmask);
+        const int idx = ((rl & (RW / 2)) ? 2 : 0) + ((rl & (RW / 4)) ? 1 : 0);
+        if ((!HALF || role == 0) && (rl & (RW / 4 - 1)) == 0 && k + idx < m) dA[q0 + k + idx] = r;
       }
     }
   }
