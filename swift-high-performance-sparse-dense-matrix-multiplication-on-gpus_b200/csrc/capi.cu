@@ -26,7 +26,8 @@ size_t plan_device_bytes(const Plan &p) {
                           &p.tile_depth, &p.tile_tall, &p.tile_format, &p.sortrowidx, &p.sortval,
                           &p.reside_ptr, &p.reside_row, &p.reside_val, &p.colorblk, &p.blkstart,
                           &p.blkstop, &p.blkptr, &p.rowcopy_b, &p.rowcopy_c, &p.g_row, &p.g_col,
-                          &p.g_val, &p.band_tiles, &p.band_ptr, &p.band_idx, &p.band_val, &p.band_dst};
+                          &p.g_val, &p.band_tiles, &p.band_ptr, &p.band_idx, &p.band_val, &p.band_dst,
+                          &p.band_mma};
   size_t s = 0;
   for (const DevBuf *b : bufs) s += b->bytes;
   for (const RowLayout *L : {&p.fwd, &p.bwd, &p.band_rest}) {

@@ -208,6 +208,10 @@ struct Plan {
   long long band_hist[129] = {};
   bool band_built = false;
   DevBuf band_tiles, band_ptr, band_idx, band_val, band_dst;
+  // the tiles in the tensor-core kernel's A-fragment order (BF16 B): 16-row windows, each value
+  // split into BF16 hi + lo parts (built on the first BF16 product after a build or refill)
+  DevBuf band_mma;
+  bool band_mma_built = false;
   RowLayout band_rest;
   std::mutex mu;  // guards lazily built layouts and scratch growth
   // Streams this plan's work was enqueued on, each with an event recorded after its latest

@@ -324,6 +324,195 @@ __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_const
   }
 }
 
+// ---------------------------------------------------------------- tensor-core tiles (BF16 B)
+// For BF16 B the tiles run on the tensor cores.  A 16-row group h pairs the 8-row tiles 2h and
+// 2h + 1 in one 16 x TWM window starting at column 16h - W (tile 2h at window columns [0, TW),
+// tile 2h + 1 at [8, 8 + TW); TWM = 8 + TW rounded up to 16), multiplied with mma.sync m16n8k16
+// (BF16 inputs, FP32 accumulation) against the B rows of the window.  Each FP32 tile value is
+// split into hi + lo BF16 parts (hi = value rounded to BF16, lo = the remainder rounded), so A
+// keeps about 16 significant bits and the products are summed in FP32.  (FP16 B keeps the
+// CUDA-core kernel: FP32 values above 65504 do not fit an FP16 hi part.)
+//
+// The window values are stored in the mma's A-fragment order: per 64-row block, per 16-row group
+// (4), per 16-column k-step (KS = TWM / 16), per part (hi, lo), 32 lanes x 16 bytes -- lane
+// l = 4g + t holds rows g and g + 8 at columns 2t, 2t + 1, 2t + 8, 2t + 9 of the k-step.  One
+// block's values are one contiguous bulk copy, and each lane reads its fragment with one
+// conflict-free 16-byte shared load.
+constexpr int mma_width(int tw) { return (kGroup + tw + 15) / 16 * 16; }  // TWM
+constexpr int kFragBytes = 32 * 16;                                      // one 16 x 16 fragment
+
+__global__ void band_mma_fill_kernel(const float *__restrict__ tiles, int nblocks, int TW, int KS,
+                                     uint4 *__restrict__ frags) {
+  const int64_t total = (int64_t)nblocks * 4 * KS * 32;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = (int)(e & 31);
+    const int64_t q = e >> 5;  // (block, group, k-step)
+    const int s = (int)(q % KS);
+    const int64_t bg = q / KS;  // block * 4 + group
+    const int g = lane >> 2, t = lane & 3;
+    const int64_t r0 = bg * 16 + g;  // rows r0 (tile 2h, window column = tile column) and r0 + 8
+    __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      // element order of the fragment: (r0, c) (r0, c+1) (r0+8, c) (r0+8, c+1) then c + 8
+      const int c = 16 * s + 2 * t + (x & 1) + ((x & 4) ? 8 : 0);
+      const int64_t r = r0 + ((x & 2) ? 8 : 0);
+      const int tc = c - ((x & 2) ? kGroup : 0);
+      const float v = (tc >= 0 && tc < TW) ? tiles[r * TW + tc] : 0.f;
+      hi[x] = __float2bfloat16_rn(v);
+      lo[x] = __float2bfloat16_rn(v - __bfloat162float(hi[x]));
+    }
+    frags[q * 64 + lane] = *reinterpret_cast<const uint4 *>(hi);
+    frags[q * 64 + 32 + lane] = *reinterpret_cast<const uint4 *>(lo);
+  }
+}
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(addr));
+}
+
+// acc += A (16 x 16, row-major fragment) x B (16 x 8, column fragment), BF16 in, FP32 accumulation
+__device__ __forceinline__ void mma_bf16(float (&acc)[4], const uint4 &a, uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+               "{%0, %1, %2, %3};"
+               : "+f"(acc[0]), "+f"(acc[1]), "+f"(acc[2]), "+f"(acc[3])
+               : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+// C[rows, this 128-column slice] += tiles x B on the tensor cores; the same persistent walk as
+// band_tile_kernel (ring of 64-row B chunks one group ahead, values double-buffered, bounded
+// waits).  Each chunk arrives as two 64-column TMA boxes with the 128-byte swizzle: 16-byte unit
+// u of ring row r sits at unit u ^ (r & 7) of its 128-byte row, so the eight row addresses of an
+// ldmatrix hit eight different bank groups.  Warp w computes the 16-row group w & 3 over the
+// 64 columns (w >> 2): eight n-tiles, each one mma per part and k-step.
+template <int TW, int MINB>
+__global__ void __launch_bounds__(256, MINB) band_mma_kernel(const __grid_constant__ CUtensorMap bmap,
+                                                             const uint4 *__restrict__ frags, int M, int N, int W,
+                                                             int ngroups, int per_block,
+                                                             __nv_bfloat16 *__restrict__ C, int64_t ldc) {
+  constexpr int TWM = mma_width(TW);
+  constexpr int KS = TWM / 16;
+  constexpr int NCH = (kCtaRows - 16 + TWM + kChunk - 1) / kChunk;  // chunks one block's windows touch
+  constexpr int NR = NCH + 1;
+  constexpr int RING_ROWS = NR * kChunk;
+  constexpr uint32_t HALF_BYTES = (uint32_t)kChunk * 128;             // 64 rows x 64 BF16 columns
+  constexpr uint32_t CHUNK_BYTES = 2 * HALF_BYTES;
+  constexpr uint32_t VAL_BYTES = (uint32_t)4 * KS * 2 * kFragBytes;   // one 64-row block
+  extern __shared__ unsigned char sm_raw[];
+  // the 128-byte swizzle repeats every 1024 bytes: align the ring to that
+  unsigned char *sm = sm_raw + ((1024u - (smem_addr(sm_raw) & 1023u)) & 1023u);
+  unsigned char *ring = sm;
+  const uint4 *vals = reinterpret_cast<const uint4 *>(sm + NR * CHUNK_BYTES);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NR * CHUNK_BYTES + 2 * VAL_BYTES);
+  const int g0 = blockIdx.x * per_block;
+  const int g1 = min(g0 + per_block, ngroups);
+  if (g0 >= g1) return;
+  const int nb = g1 - g0, nchunks = nb - 1 + NCH;
+  const int col0 = blockIdx.y * kSlice;
+  const int rbase = g0 * kCtaRows - W;
+  int issued_chunks = 0, issued_vals = 0;  // producer (thread 0) state
+  auto issue_chunk = [&](int c) {
+    const uint32_t b = smem_addr(bar + c % NR);
+    const uint32_t dst = smem_addr(ring + (size_t)(c % NR) * CHUNK_BYTES);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(CHUNK_BYTES) : "memory");
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf)
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+          "[%4];" ::"r"(dst + hf * HALF_BYTES),
+          "l"(reinterpret_cast<uint64_t>(&bmap)), "r"(col0 + 64 * hf), "r"(rbase + kChunk * c), "r"(b)
+          : "memory");
+    issued_chunks = c + 1;
+  };
+  auto issue_vals = [&](int k) {
+    const uint32_t b = smem_addr(bar + NR + (k & 1));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(VAL_BYTES) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(vals + (size_t)(k & 1) * (VAL_BYTES / 16))),
+                 "l"(frags + (size_t)(g0 + k) * (VAL_BYTES / 16)), "r"(VAL_BYTES), "r"(b)
+                 : "memory");
+    issued_vals = k + 1;
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NR + 2; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar + s)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int c = 0; c < NR && c < nchunks; ++c) issue_chunk(c);
+    for (int k = 0; k < 2 && k < nb; ++k) issue_vals(k);
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = w & 3, nh = w >> 2;
+  const int g = lane >> 2, t = lane & 3;
+  const int cb = col0 + 64 * nh + 2 * t;  // this lane's first column (n-tile j adds 8j)
+  // ldmatrix.trans addresses: lanes 0-15 give k rows 0-15 of n-tile 2jj, lanes 16-31 of 2jj + 1
+  const int lrow = lane & 15, lunit = lane >> 4;
+  const uint32_t ring_s = smem_addr(ring) + nh * HALF_BYTES;
+  for (int k = 0; k < nb; ++k) {
+    const int rw = (g0 + k) * kCtaRows + 16 * grp + g;  // C rows rw and rw + 8
+    // the rest walk's C values, kept packed until the end so that no mma waits on them
+    uint32_t old[8][2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = rw + 8 * h, c = cb + 8 * j;
+        old[j][h] = (r < M && c < N) ? __ldcs(reinterpret_cast<const unsigned int *>(C + (int64_t)r * ldc + c)) : 0u;
+      }
+    float acc[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < NCH; ++j) bad |= !wait_phase(smem_addr(bar + (k + j) % NR), (uint32_t)(((k + j) / NR) & 1));
+    bad |= !wait_phase(smem_addr(bar + NR + (k & 1)), (uint32_t)((k >> 1) & 1));
+    if (__syncthreads_or(bad)) {
+      if (threadIdx.x == 0) {
+        atomicExch(&g_band_timeout, 1);
+        // give the copies still in flight a bounded chance to land before the block leaves
+        for (int c = max(0, issued_chunks - NR); c < issued_chunks; ++c)
+          wait_phase(smem_addr(bar + c % NR), (uint32_t)((c / NR) & 1));
+        for (int v = max(0, issued_vals - 2); v < issued_vals; ++v)
+          wait_phase(smem_addr(bar + NR + (v & 1)), (uint32_t)((v >> 1) & 1));
+      }
+      return;
+    }
+    const uint4 *A = vals + (size_t)(k & 1) * (VAL_BYTES / 16) + (size_t)grp * KS * 64 + lane;
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+      const uint4 ahi = A[s * 64], alo = A[s * 64 + 32];
+      int rr = (k % NR) * kChunk + 16 * grp + 16 * s + lrow;  // ring row of this lane's address
+      if (rr >= RING_ROWS) rr -= RING_ROWS;                      // 16-row steps never straddle the wrap
+      const uint32_t rowaddr = ring_s + (uint32_t)(rr / kChunk) * CHUNK_BYTES + (uint32_t)(rr % kChunk) * 128;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        uint32_t b0, b1, b2, b3;
+        ldsm_x4_trans(rowaddr + ((uint32_t)((2 * jj + lunit) ^ (rr & 7)) << 4), b0, b1, b2, b3);
+        mma_bf16(acc[2 * jj], ahi, b0, b1);
+        mma_bf16(acc[2 * jj + 1], ahi, b2, b3);
+        mma_bf16(acc[2 * jj], alo, b0, b1);
+        mma_bf16(acc[2 * jj + 1], alo, b2, b3);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = rw + 8 * h, c = cb + 8 * j;
+        if (r < M && c < N) {
+          const float2 o = unpack2<__nv_bfloat16>(old[j][h]);
+          const __nv_bfloat162 v = __floats2bfloat162_rn(acc[j][2 * h] + o.x, acc[j][2 * h + 1] + o.y);
+          *reinterpret_cast<__nv_bfloat162 *>(C + (int64_t)r * ldc + c) = v;
+        }
+      }
+    __syncthreads();  // chunk k's slot and value slot k & 1 are free again
+    if (threadIdx.x == 0) {
+      if (k + NR < nchunks) issue_chunk(k + NR);
+      if (k + 2 < nb) issue_vals(k + 2);
+    }
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void *f = nullptr;
@@ -374,6 +563,41 @@ swift_status launch_tile_w(const CUtensorMap &map, const float *tiles, int M, in
   return SWIFT_ERR_UNSUPPORTED;
 }
 
+template <int TW>
+swift_status launch_mma(const CUtensorMap &map, const uint4 *frags, int M, int N, int W, void *C, int64_t ldc,
+                        int sm_count, cudaStream_t st) {
+  constexpr int KS = mma_width(TW) / 16;
+  constexpr int NR = (kCtaRows - 16 + mma_width(TW) + kChunk - 1) / kChunk + 1;
+  constexpr size_t smem = (size_t)NR * 2 * kChunk * 128 + 2 * (size_t)4 * KS * 2 * kFragBytes + (NR + 2) * 8 + 1024;
+  constexpr int minb = smem * 2 + 2048 <= 227 * 1024 ? 2 : 1;
+  static_assert(smem <= 227 * 1024, "band mma kernel: shared memory above the per-block limit");
+  auto k = band_mma_kernel<TW, minb>;
+  SW_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  SW_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem));
+  const int ngroups = (M + kCtaRows - 1) / kCtaRows, nslices = (N + kSlice - 1) / kSlice;
+  int ranges = std::max(1, std::min(ngroups, sm_count * std::max(occ, 1) / nslices));
+  const int per = (ngroups + ranges - 1) / ranges;
+  ranges = (ngroups + per - 1) / per;
+  k<<<dim3((unsigned)ranges, (unsigned)nslices), 256, smem, st>>>(map, frags, M, N, W, ngroups, per,
+                                                                 static_cast<__nv_bfloat16 *>(C), ldc);
+  SW_CHECK_LAUNCH();
+  return SWIFT_OK;
+}
+
+swift_status launch_mma_w(const CUtensorMap &map, const uint4 *frags, int M, int N, int W, void *C, int64_t ldc,
+                          int sm_count, cudaStream_t st) {
+  switch (W) {
+    case 3: return launch_mma<tile_width(3)>(map, frags, M, N, W, C, ldc, sm_count, st);
+    case 7: return launch_mma<tile_width(7)>(map, frags, M, N, W, C, ldc, sm_count, st);
+    case 15: return launch_mma<tile_width(15)>(map, frags, M, N, W, C, ldc, sm_count, st);
+    case 31: return launch_mma<tile_width(31)>(map, frags, M, N, W, C, ldc, sm_count, st);
+    case 47: return launch_mma<tile_width(47)>(map, frags, M, N, W, C, ldc, sm_count, st);
+    case 63: return launch_mma<tile_width(63)>(map, frags, M, N, W, C, ldc, sm_count, st);
+  }
+  return SWIFT_ERR_UNSUPPORTED;
+}
+
 }  // namespace
 
 // Distance profile and the half-width choice (p.mu held).
@@ -417,6 +641,7 @@ static swift_status band_build(Plan &p, int W, cudaStream_t st) {
   const int64_t rows_pad = (int64_t)((p.M + kCtaRows - 1) / kCtaRows) * kCtaRows;
   if (rows_pad * TW >= INT32_MAX) return SWIFT_ERR_OVERFLOW;
   p.band_built = false;
+  p.band_mma_built = false;
   SW_TRY(p.band_tiles.alloc(sizeof(float) * (size_t)std::max<int64_t>(rows_pad * TW, 1)));
   SW_CHECK_CUDA(cudaMemsetAsync(p.band_tiles.p, 0, p.band_tiles.bytes, st));
   SW_TRY(p.band_ptr.alloc(sizeof(int) * ((size_t)p.M + 1)));
@@ -456,8 +681,23 @@ static swift_status band_build(Plan &p, int W, cudaStream_t st) {
   return SWIFT_OK;
 }
 
+// The tiles in the tensor-core kernel's fragment order (p.mu held; after band_build).
+static swift_status band_mma_build(Plan &p, cudaStream_t st) {
+  const int TW = tile_width(p.band_used_w);
+  const int KS = mma_width(TW) / 16;
+  const int nblocks = (p.M + kCtaRows - 1) / kCtaRows;
+  SW_TRY(p.band_mma.alloc((size_t)std::max(nblocks, 1) * 4 * KS * 2 * kFragBytes));
+  const int64_t threads = (int64_t)nblocks * 4 * KS * 32;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)p.sm_count * 16));
+  band_mma_fill_kernel<<<grid, 256, 0, st>>>(p.band_tiles.as<float>(), nblocks, TW, KS, p.band_mma.as<uint4>());
+  SW_CHECK_LAUNCH();
+  p.band_mma_built = true;
+  return SWIFT_OK;
+}
+
 swift_status band_refill(Plan &p, cudaStream_t st) {
   if (!p.band_built || p.nnz == 0) return SWIFT_OK;
+  p.band_mma_built = false;  // regrouped on the next BF16 product
   const int grid = (int)std::min<int64_t>(((int64_t)p.nnz + 255) / 256, (int64_t)p.sm_count * 16);
   if (p.val_type == SWIFT_F64)
     band_refill_kernel<double><<<grid, 256, 0, st>>>(p.val.as<double>(), p.nnz, p.band_dst.as<int>(),
@@ -490,6 +730,7 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
     SW_TRY(band_profile(p, st));
     W = p.band_w >= 0 ? p.band_w : kWidths[0];
     if (!p.band_built || p.band_used_w != W) SW_TRY(band_build(p, W, st));
+    if (d.dtype == SWIFT_BF16 && !p.band_mma_built) SW_TRY(band_mma_build(p, st));
   }
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) {
@@ -500,13 +741,17 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
   CUtensorMap map;
   cuuint64_t dims[2] = {(cuuint64_t)d.N, (cuuint64_t)std::max(p.K, 1)};
   cuuint64_t strides[1] = {(cuuint64_t)(d.ldb * (int64_t)esz)};
-  cuuint32_t box[2] = {(cuuint32_t)kSlice, (cuuint32_t)kChunk};
+  // BF16 (tensor-core kernel): two 64-column boxes per chunk, 128-byte swizzle; else one
+  // 128-column box, unswizzled
+  const bool mma = d.dtype == SWIFT_BF16;
+  cuuint32_t box[2] = {(cuuint32_t)(mma ? 64 : kSlice), (cuuint32_t)kChunk};
   cuuint32_t es[2] = {1, 1};
   const CUtensorMapDataType dt = d.dtype == SWIFT_F32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : d.dtype == SWIFT_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                          : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   const CUresult cr = enc(&map, dt, 2, const_cast<void *>(d.B), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          mma ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) {
     set_last_error("cuTensorMapEncodeTiled", "B cannot be described as a TMA tensor");
@@ -517,7 +762,8 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
   const float *tiles = p.band_tiles.as<float>();
   switch (d.dtype) {
     case SWIFT_F32: return launch_tile_w<float>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
-    case SWIFT_BF16: return launch_tile_w<__nv_bfloat16>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
+    case SWIFT_BF16:
+      return launch_mma_w(map, p.band_mma.as<uint4>(), p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
     case SWIFT_F16: return launch_tile_w<__half>(map, tiles, p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
     default: return SWIFT_ERR_UNSUPPORTED;
   }

@@ -214,3 +214,50 @@ def test_band_no_timeouts():
     f = C.c_int(-1)
     capi.check(capi.lib().swift_band_timeout_flag(C.byref(f), 0), "swift_band_timeout_flag")
     assert f.value == 0
+
+
+@pytest.mark.parametrize("N", [128, 136, 200, 256])  # BF16 rows a multiple of 16 bytes
+@pytest.mark.parametrize("shape", [(1000, 1000, 32), (1500, 1000, 16), (777, 1200, 4), (4096, 4096, 48)])
+def test_band_bf16_tensor_core_exact(shape, N):
+    """BF16 B runs the tiles on the tensor cores.  With integer A in {-1, 1} and B in {-2..2}
+    every partial and total sum is an integer below 256, exact in FP32 and in BF16, so C must
+    equal the FP64 product bit for bit: a value in the wrong fragment slot, B row or column
+    would show."""
+    M, K, half = shape
+    rp, ci = band_pattern(M, K, half, 0.002, seed=half)
+    rng = np.random.default_rng(half + N)
+    val = rng.choice(np.array([-1.0, 1.0], np.float32), len(ci))
+    Bi = rng.integers(-2, 3, (K, N)).astype(np.float32)
+    B = torch.from_numpy(Bi).cuda().to(torch.bfloat16)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    C = pl.spmm(B, engine="band")
+    torch.cuda.synchronize()
+    ref = pl.spmm_f64_reference(B.double()).cpu().numpy()
+    assert np.abs(ref).max() < 256
+    assert pl.band_profile()[1] >= 0  # the band engine chose a tile width
+    assert np.array_equal(C.double().cpu().numpy(), ref)
+    pl.close()
+
+
+def test_band_bf16_keeps_fp32_values():
+    """A's FP32 values reach the tensor cores as BF16 hi + lo parts: rows holding 1 + 3 * 2^-12
+    and -1 against equal B rows must give 3 * 2^-12 (the hi parts alone would give 0)."""
+    M = K = 512
+    i = np.arange(M - 1, dtype=np.int64)
+    rp, ci = gen.coo_to_csr(M, np.concatenate([i, i]), np.concatenate([i, i + 1]), K=K)
+    rows = np.repeat(np.arange(M), np.diff(rp))
+    val = np.where(ci == rows, np.float32(1 + 3 * 2.0 ** -12), np.float32(-1.0)).astype(np.float32)
+    B = torch.ones(K, 128, device="cuda", dtype=torch.bfloat16)
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    C = pl.spmm(B, engine="band")
+    torch.cuda.synchronize()
+    expect = np.full((M, 128), 3 * 2.0 ** -12)
+    expect[M - 1] = 0.0
+    assert np.array_equal(C.double().cpu().numpy(), expect)
+    # new values for the same pattern reach the tensor cores too (the fragments are rebuilt)
+    pl.set_values(np.where(val < 0, val, np.float32(1 + 5 * 2.0 ** -12)).astype(np.float32))
+    C = pl.spmm(B, engine="band")
+    torch.cuda.synchronize()
+    expect[:M - 1] = 5 * 2.0 ** -12
+    assert np.array_equal(C.double().cpu().numpy(), expect)
+    pl.close()
