@@ -53,6 +53,7 @@ WORKLOADS = {
     "rmat19band_n128_f32": dict(kind="rmatband", scale=19, edges=16 << 20, N=128, dtype="f32"),
     # half-size banded case for full ncu captures of the band engine (B and C exceed L2)
     "rmat18band_n128_f32": dict(kind="rmatband", scale=18, edges=8 << 20, N=128, dtype="f32"),
+    "rmat18band_n128_bf16": dict(kind="rmatband", scale=18, edges=8 << 20, N=128, dtype="bf16"),
     # precision ratios (FP32 vs BF16 vs FP16 B/C on one FP32-valued matrix)
     "precision_rmat19band_n128": dict(kind="precision", rk="rmatband", scale=19, edges=16 << 20, N=128),
     # differentiation: GNN layer on a symmetric-normalised R-MAT graph, fused vs plain
@@ -492,11 +493,15 @@ def run_precision(args):
         rest_nnz = int(np.count_nonzero((cols < c0) | (cols >= c0 + tw)))
         del rows, c0, cols
         tile_bytes = ((M + 63) // 64) * 64 * tw * 4
-        band = {"half_width": bw, "tile_width": tw, "tile_bytes": tile_bytes, "rest_nnz": rest_nnz,
-                "in_tiles_nnz": nnz - rest_nnz}
+        # BF16 B runs the tiles on the tensor cores: 16-row windows of 8 + tw columns rounded up
+        # to 16, each value as BF16 hi + lo parts (4 bytes)
+        twm = (8 + tw + 15) // 16 * 16
+        mma_bytes = ((M + 63) // 64) * 64 * twm * 4
+        band = {"half_width": bw, "tile_width": tw, "tile_bytes": tile_bytes, "mma_window_width": twm,
+                "mma_fragment_bytes": mma_bytes, "rest_nnz": rest_nnz, "in_tiles_nnz": nnz - rest_nnz}
         for name in ("f32", "bf16", "f16"):
             esz = 4 if name == "f32" else 2
-            b = tile_bytes + rest_nnz * 8 + (K + M) * N * esz
+            b = (mma_bytes if name == "bf16" else tile_bytes) + rest_nnz * 8 + (K + M) * N * esz
             band[f"format_bytes_{name}"] = b
             if res[name]["engine"] == "band":
                 res[name]["algorithmic_bytes_band_format"] = b
@@ -528,7 +533,7 @@ def run_precision(args):
         "byte_model_ceiling_16bit_vs_f32": f32b / bfb,
         "band_format": band,
         "roofline": roofline_line(res["bf16"].get("algorithmic_bytes_band_format", bfb), res["bf16"]["ms"],
-                                  args.workload, "band_tile_kernel + merge_flag_kernel" if res["bf16"]["engine"] == "band"
+                                  args.workload, "band_mma_kernel + merge_flag_kernel" if res["bf16"]["engine"] == "band"
                                   else "merge_flag_kernel"),
         "products": res,
         "gpu_launches": args.steps,

@@ -208,10 +208,12 @@ struct Plan {
   long long band_hist[129] = {};
   bool band_built = false;
   DevBuf band_tiles, band_ptr, band_idx, band_val, band_dst;
-  // the tiles in the tensor-core kernel's A-fragment order (BF16 B): 16-row windows, each value
-  // split into BF16 hi + lo parts (built on the first BF16 product after a build or refill)
+  // the tiles in the tensor-core kernel's A-fragment order (16-bit B): 16-row windows, each row
+  // scaled by a power of two and split into hi + lo parts of B's type, then the rows' inverse
+  // factors; band_mma_dtype is the type they were built for (-1: none; rebuilt on the first
+  // 16-bit product after a build, a refill or a change of type)
   DevBuf band_mma;
-  bool band_mma_built = false;
+  int band_mma_dtype = -1;
   RowLayout band_rest;
   std::mutex mu;  // guards lazily built layouts and scratch growth
   // Streams this plan's work was enqueued on, each with an event recorded after its latest

@@ -216,19 +216,20 @@ def test_band_no_timeouts():
     assert f.value == 0
 
 
-@pytest.mark.parametrize("N", [128, 136, 200, 256])  # BF16 rows a multiple of 16 bytes
+@pytest.mark.parametrize("dt", ["bfloat16", "float16"])
+@pytest.mark.parametrize("N", [128, 136, 200, 256])  # 16-bit rows a multiple of 16 bytes
 @pytest.mark.parametrize("shape", [(1000, 1000, 32), (1500, 1000, 16), (777, 1200, 4), (4096, 4096, 48)])
-def test_band_bf16_tensor_core_exact(shape, N):
-    """BF16 B runs the tiles on the tensor cores.  With integer A in {-1, 1} and B in {-2..2}
-    every partial and total sum is an integer below 256, exact in FP32 and in BF16, so C must
-    equal the FP64 product bit for bit: a value in the wrong fragment slot, B row or column
-    would show."""
+def test_band_16bit_tensor_core_exact(shape, N, dt):
+    """16-bit B runs the tiles on the tensor cores.  With integer A in {-1, 1} and B in {-2..2}
+    every partial and total sum is an integer below 256, exact in FP32, BF16 and FP16, so C must
+    equal the FP64 product bit for bit: a value in the wrong fragment slot, B row or column, or
+    a wrong row factor would show."""
     M, K, half = shape
     rp, ci = band_pattern(M, K, half, 0.002, seed=half)
     rng = np.random.default_rng(half + N)
     val = rng.choice(np.array([-1.0, 1.0], np.float32), len(ci))
     Bi = rng.integers(-2, 3, (K, N)).astype(np.float32)
-    B = torch.from_numpy(Bi).cuda().to(torch.bfloat16)
+    B = torch.from_numpy(Bi).cuda().to(getattr(torch, dt))
     pl = Plan.from_csr(rp, ci, val, (M, K))
     C = pl.spmm(B, engine="band")
     torch.cuda.synchronize()
@@ -239,15 +240,17 @@ def test_band_bf16_tensor_core_exact(shape, N):
     pl.close()
 
 
-def test_band_bf16_keeps_fp32_values():
-    """A's FP32 values reach the tensor cores as BF16 hi + lo parts: rows holding 1 + 3 * 2^-12
-    and -1 against equal B rows must give 3 * 2^-12 (the hi parts alone would give 0)."""
+@pytest.mark.parametrize("dt", ["bfloat16", "float16"])
+def test_band_16bit_keeps_fp32_values(dt):
+    """A's FP32 values reach the tensor cores as hi + lo parts of B's type: rows holding
+    1 + 3 * 2^-12 and -1 against equal B rows must give 3 * 2^-12 (the hi parts alone would give
+    0 in BF16 and 2^-10 in FP16)."""
     M = K = 512
     i = np.arange(M - 1, dtype=np.int64)
     rp, ci = gen.coo_to_csr(M, np.concatenate([i, i]), np.concatenate([i, i + 1]), K=K)
     rows = np.repeat(np.arange(M), np.diff(rp))
     val = np.where(ci == rows, np.float32(1 + 3 * 2.0 ** -12), np.float32(-1.0)).astype(np.float32)
-    B = torch.ones(K, 128, device="cuda", dtype=torch.bfloat16)
+    B = torch.ones(K, 128, device="cuda", dtype=getattr(torch, dt))
     pl = Plan.from_csr(rp, ci, val, (M, K))
     C = pl.spmm(B, engine="band")
     torch.cuda.synchronize()
@@ -260,4 +263,23 @@ def test_band_bf16_keeps_fp32_values():
     torch.cuda.synchronize()
     expect[:M - 1] = 5 * 2.0 ** -12
     assert np.array_equal(C.double().cpu().numpy(), expect)
+    pl.close()
+
+
+def test_band_fp16_rows_beyond_fp16_range():
+    """FP16 B with A rows of magnitude 1e5 (beyond FP16's 65504), 1 and 0.1: each row is scaled
+    by a power of two before its FP16 split, so C stays finite and within FP16 output rounding of
+    the FP64 product, row by row."""
+    M = K = 2048
+    rp, ci = band_pattern(M, K, 16)  # every nonzero in the tiles (no rest)
+    rows = np.repeat(np.arange(M), np.diff(rp))
+    mag = np.where(rows % 3 == 0, 1e5, np.where(rows % 3 == 1, 1.0, 0.1)).astype(np.float32)
+    val = (gen.uniform_values(len(ci), seed=5) * mag).astype(np.float32)
+    B = (torch.from_numpy(gen.dense_uniform(K, 128, seed=6)).cuda() * 2.0 ** -6).half()
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    C = pl.spmm(B, engine="band").double().cpu().numpy()
+    ref = pl.spmm_f64_reference(B.double()).cpu().numpy()
+    assert np.isfinite(C).all()
+    err = np.abs(C - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert err.max() <= 1e-3, err.max()
     pl.close()
