@@ -493,15 +493,15 @@ def run_precision(args):
         rest_nnz = int(np.count_nonzero((cols < c0) | (cols >= c0 + tw)))
         del rows, c0, cols
         tile_bytes = ((M + 63) // 64) * 64 * tw * 4
-        # BF16 B runs the tiles on the tensor cores: 16-row windows of 8 + tw columns rounded up
-        # to 16, each value as BF16 hi + lo parts (4 bytes)
+        # 16-bit B runs the tiles on the tensor cores: 16-row windows of 8 + tw columns rounded up
+        # to 16, each value as hi + lo parts of B's type (4 bytes), plus one FP32 row factor per row
         twm = (8 + tw + 15) // 16 * 16
-        mma_bytes = ((M + 63) // 64) * 64 * twm * 4
+        mma_bytes = ((M + 63) // 64) * 64 * (twm * 4 + 4)
         band = {"half_width": bw, "tile_width": tw, "tile_bytes": tile_bytes, "mma_window_width": twm,
                 "mma_fragment_bytes": mma_bytes, "rest_nnz": rest_nnz, "in_tiles_nnz": nnz - rest_nnz}
         for name in ("f32", "bf16", "f16"):
             esz = 4 if name == "f32" else 2
-            b = (mma_bytes if name == "bf16" else tile_bytes) + rest_nnz * 8 + (K + M) * N * esz
+            b = (tile_bytes if name == "f32" else mma_bytes) + rest_nnz * 8 + (K + M) * N * esz
             band[f"format_bytes_{name}"] = b
             if res[name]["engine"] == "band":
                 res[name]["algorithmic_bytes_band_format"] = b
