@@ -435,7 +435,7 @@ __device__ __forceinline__ void stsm_x4(uint32_t addr, uint32_t r0, uint32_t r1,
 // acc += A (16 x 16, row-major fragment) x B (16 x 8, column fragment), 16-bit in, FP32 accumulation
 template <class T>
 __device__ __forceinline__ void mma16(float (&acc)[4], const uint4 &a, uint32_t b0, uint32_t b1) {
-  if constexpr (sizeof(T) == 2 && std::is_same<T, __nv_bfloat16>::value) {
+  if constexpr (std::is_same<T, __nv_bfloat16>::value) {
     asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
                  "{%0, %1, %2, %3};"
                  : "+f"(acc[0]), "+f"(acc[1]), "+f"(acc[2]), "+f"(acc[3])

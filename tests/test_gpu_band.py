@@ -216,14 +216,14 @@ def test_band_no_timeouts():
     assert f.value == 0
 
 
-@pytest.mark.parametrize("dt", ["bfloat16", "float16"])
+@pytest.mark.parametrize("dt", ["float32", "bfloat16", "float16"])
 @pytest.mark.parametrize("N", [128, 136, 200, 256])  # 16-bit rows a multiple of 16 bytes
 @pytest.mark.parametrize("shape", [(1000, 1000, 32), (1500, 1000, 16), (777, 1200, 4), (4096, 4096, 48)])
-def test_band_16bit_tensor_core_exact(shape, N, dt):
-    """16-bit B runs the tiles on the tensor cores.  With integer A in {-1, 1} and B in {-2..2}
-    every partial and total sum is an integer below 256, exact in FP32, BF16 and FP16, so C must
-    equal the FP64 product bit for bit: a value in the wrong fragment slot, B row or column, or
-    a wrong row factor would show."""
+def test_band_tensor_core_exact(shape, N, dt):
+    """16-bit B runs the tiles on the tensor cores (hi + lo parts), FP32 B on CUDA cores.  With
+    integer A in {-1, 1} and B in {-2..2} every partial and total sum is an integer below 256,
+    exact in FP32, BF16 and FP16, so C must equal the FP64 product bit for bit: a value in the
+    wrong fragment slot, B row or column, or a wrong row factor would show."""
     M, K, half = shape
     rp, ci = band_pattern(M, K, half, 0.002, seed=half)
     rng = np.random.default_rng(half + N)
@@ -282,4 +282,16 @@ def test_band_fp16_rows_beyond_fp16_range():
     assert np.isfinite(C).all()
     err = np.abs(C - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert err.max() <= 1e-3, err.max()
+    pl.close()
+
+
+def test_band_fp32_accuracy():
+    """FP32 B: the tiles' product stays within a few FP32 roundings of the FP64 product (the row
+    walk alone reaches about 5e-7 on this matrix)."""
+    M, K, rp, ci, val = build("band32_plus_rmat")
+    B = torch.from_numpy(gen.dense_uniform(K, 128, seed=17)).cuda()
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    C = pl.spmm(B, engine="band")
+    ref = pl.spmm_f64_reference(B.double()).cpu().numpy()
+    assert relerr(C.cpu().numpy(), ref) <= 2e-6
     pl.close()
