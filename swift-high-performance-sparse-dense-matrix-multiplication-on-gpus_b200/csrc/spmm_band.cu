@@ -149,58 +149,6 @@ __global__ void band_refill_kernel(const TV *__restrict__ val, int64_t nnz, cons
   }
 }
 
-template <class T>
-__device__ __forceinline__ void load4(const T *p, float (&o)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 f = *reinterpret_cast<const float4 *>(p);
-    o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
-  } else {
-    const uint2 u = *reinterpret_cast<const uint2 *>(p);
-    const float2 a = unpack2<T>(u.x), b = unpack2<T>(u.y);
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void store4(T *p, const float (&v)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    __stcs(reinterpret_cast<float4 *>(p), make_float4(v[0], v[1], v[2], v[3]));
-  } else {
-    T h[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) h[k] = from_acc<T>(v[k]);
-    *reinterpret_cast<uint2 *>(p) = *reinterpret_cast<const uint2 *>(h);
-  }
-}
-
-// Four consecutive C elements held in their storage type (streaming load, evict-first).
-template <class T>
-struct Packed4 {
-  uint32_t u[sizeof(T)];  // 4 x 4 bytes (FP32) or 2 x 4 bytes (16-bit)
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int i = 0; i < (int)sizeof(T); ++i) u[i] = 0u;
-  }
-  __device__ __forceinline__ void load_stream(const T *p) {
-    if constexpr (sizeof(T) == 4) {
-      const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(p));
-      u[0] = q.x; u[1] = q.y; u[2] = q.z; u[3] = q.w;
-    } else {
-      const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(p));
-      u[0] = q.x; u[1] = q.y;
-    }
-  }
-  __device__ __forceinline__ void unpack(float (&o)[4]) const {
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) o[i] = __uint_as_float(u[i]);
-    } else {
-      const float2 a = unpack2<T>(u[0]), b = unpack2<T>(u[1]);
-      o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-    }
-  }
-};
-
 // C[rows, this 128-column slice] += tiles x B, one persistent block per contiguous range of
 // 64-row groups.  The B rows a group's tiles touch (64 + TW - 8 of them, starting W rows above
 // the group) overlap the next group's by TW - 8 rows, so B lives in a ring of 64-row chunks:
@@ -210,19 +158,19 @@ struct Packed4 {
 // loads fill the ring (rows outside B are zero-filled), bulk copies the values, one mbarrier
 // per slot.  The old C rows (the rest walk's result) are loaded into registers before the
 // waits.  Waits are bounded; a block that gives up sets g_band_timeout and leaves.
-template <class T, int TW, int MINB>
+template <int TW, int MINB>
 __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_constant__ CUtensorMap bmap,
                                                               const float *__restrict__ tiles, int M, int N, int W,
-                                                              int ngroups, int per_block, T *__restrict__ C,
+                                                              int ngroups, int per_block, float *__restrict__ C,
                                                               int64_t ldc) {
   constexpr int PR = panel_rows(TW);
   constexpr int NCH = (PR + kChunk - 1) / kChunk;
   constexpr int NR = NCH + 1;
   constexpr int RING_ROWS = NR * kChunk;
-  constexpr uint32_t CHUNK_BYTES = (uint32_t)kChunk * kSlice * sizeof(T);
+  constexpr uint32_t CHUNK_BYTES = (uint32_t)kChunk * kSlice * 4;
   constexpr uint32_t VAL_BYTES = (uint32_t)kCtaRows * TW * 4;
   extern __shared__ __align__(1024) unsigned char sm[];
-  T *ring = reinterpret_cast<T *>(sm);
+  float *ring = reinterpret_cast<float *>(sm);
   float *vals = reinterpret_cast<float *>(sm + NR * CHUNK_BYTES);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NR * CHUNK_BYTES + 2 * VAL_BYTES);  // NR chunks, 2 values
   const int g0 = blockIdx.x * per_block;
@@ -262,13 +210,12 @@ __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_const
   const int col = col0 + lane * 4;
   for (int k = 0; k < nb; ++k) {
     const int rw = (g0 + k) * kCtaRows + kGroup * w;  // first C row of this warp
-    // the rest walk's C rows, kept packed until the end so that no FMA waits on them
-    Packed4<T> old[kGroup];
+    // the rest walk's C rows, in their own registers so that no FMA waits on them
+    float4 old[kGroup];
 #pragma unroll
-    for (int r = 0; r < kGroup; ++r) {
-      if (rw + r < M && col < N) old[r].load_stream(C + (int64_t)(rw + r) * ldc + col);
-      else old[r].zero();
-    }
+    for (int r = 0; r < kGroup; ++r)
+      old[r] = (rw + r < M && col < N) ? __ldcs(reinterpret_cast<const float4 *>(C + (int64_t)(rw + r) * ldc + col))
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
     float acc[kGroup][4];
 #pragma unroll
     for (int r = 0; r < kGroup; ++r) acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.f;
@@ -293,10 +240,13 @@ __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_const
     for (int c = 0; c < TW; c += 4) {
       int rr = rb + c;
       if (rr >= RING_ROWS) rr -= RING_ROWS;  // four rows never straddle the wrap (all multiples of 4)
-      const T *bp = ring + (size_t)rr * kSlice + lane * 4;
+      const float *bp = ring + (size_t)rr * kSlice + lane * 4;
       float bv[4][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) load4<T>(bp + q * kSlice, bv[q]);
+      for (int q = 0; q < 4; ++q) {
+        const float4 f = *reinterpret_cast<const float4 *>(bp + q * kSlice);
+        bv[q][0] = f.x; bv[q][1] = f.y; bv[q][2] = f.z; bv[q][3] = f.w;
+      }
       float4 v[kGroup];
 #pragma unroll
       for (int r = 0; r < kGroup; ++r) v[r] = *reinterpret_cast<const float4 *>(E + r * TW + c);
@@ -312,13 +262,10 @@ __global__ void __launch_bounds__(256, MINB) band_tile_kernel(const __grid_const
     }
     if (col < N) {
 #pragma unroll
-      for (int r = 0; r < kGroup; ++r) {
-        float o[4];
-        old[r].unpack(o);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[r][e] += o[e];
-        if (rw + r < M) store4<T>(C + (int64_t)(rw + r) * ldc + col, acc[r]);
-      }
+      for (int r = 0; r < kGroup; ++r)
+        if (rw + r < M)
+          __stcs(reinterpret_cast<float4 *>(C + (int64_t)(rw + r) * ldc + col),
+                 make_float4(acc[r][0] + old[r].x, acc[r][1] + old[r].y, acc[r][2] + old[r].z, acc[r][3] + old[r].w));
     }
     __syncthreads();  // chunk k's slot and value slot k & 1 are free again
     if (threadIdx.x == 0) {
@@ -628,16 +575,15 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-template <class T, int TW>
+template <int TW>
 swift_status launch_tile(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
                          int sm_count, cudaStream_t st) {
   constexpr int NR = (panel_rows(TW) + kChunk - 1) / kChunk + 1;
-  constexpr size_t smem = (size_t)NR * kChunk * kSlice * sizeof(T) + 2 * (size_t)kCtaRows * TW * 4 + (NR + 2) * 8;
-  // two blocks per SM where shared memory allows it and the 16-bit walk's registers fit (the FP32
-  // variant keeps its old-C rows in 32 more registers and would spill at 128)
-  constexpr int minb = sizeof(T) == 2 && smem * 2 + 2048 <= 227 * 1024 ? 2 : 1;
+  constexpr size_t smem = (size_t)NR * kChunk * kSlice * 4 + 2 * (size_t)kCtaRows * TW * 4 + (NR + 2) * 8;
+  // one block per SM: its old-C rows and accumulators (64 registers) would spill at the 128
+  // registers of two blocks
   static_assert(smem <= 227 * 1024, "band tile kernel: shared memory above the per-block limit");
-  auto k = band_tile_kernel<T, TW, minb>;
+  auto k = band_tile_kernel<TW, 1>;
   SW_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   SW_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 256, smem));
@@ -647,21 +593,20 @@ swift_status launch_tile(const CUtensorMap &map, const float *tiles, int M, int 
   const int per = (ngroups + ranges - 1) / ranges;
   ranges = (ngroups + per - 1) / per;
   k<<<dim3((unsigned)ranges, (unsigned)nslices), 256, smem, st>>>(map, tiles, M, N, W, ngroups, per,
-                                                                 static_cast<T *>(C), ldc);
+                                                                 static_cast<float *>(C), ldc);
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
 }
 
-template <class T>
 swift_status launch_tile_w(const CUtensorMap &map, const float *tiles, int M, int N, int W, void *C, int64_t ldc,
                            int sm_count, cudaStream_t st) {
   switch (W) {
-    case 3: return launch_tile<T, tile_width(3)>(map, tiles, M, N, W, C, ldc, sm_count, st);
-    case 7: return launch_tile<T, tile_width(7)>(map, tiles, M, N, W, C, ldc, sm_count, st);
-    case 15: return launch_tile<T, tile_width(15)>(map, tiles, M, N, W, C, ldc, sm_count, st);
-    case 31: return launch_tile<T, tile_width(31)>(map, tiles, M, N, W, C, ldc, sm_count, st);
-    case 47: return launch_tile<T, tile_width(47)>(map, tiles, M, N, W, C, ldc, sm_count, st);
-    case 63: return launch_tile<T, tile_width(63)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 3: return launch_tile<tile_width(3)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 7: return launch_tile<tile_width(7)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 15: return launch_tile<tile_width(15)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 31: return launch_tile<tile_width(31)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 47: return launch_tile<tile_width(47)>(map, tiles, M, N, W, C, ldc, sm_count, st);
+    case 63: return launch_tile<tile_width(63)>(map, tiles, M, N, W, C, ldc, sm_count, st);
   }
   return SWIFT_ERR_UNSUPPORTED;
 }
@@ -900,7 +845,7 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
     return SWIFT_ERR_UNSUPPORTED;
   }
   SW_TRY(run_merge(p, p.band_rest, d, o, st));
-  return launch_tile_w<float>(map, p.band_tiles.as<float>(), p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
+  return launch_tile_w(map, p.band_tiles.as<float>(), p.M, d.N, W, d.C, d.ldc, p.sm_count, st);
 }
 
 swift_status band_timeout_flag(int *flag, int reset) {

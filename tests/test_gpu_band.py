@@ -208,14 +208,6 @@ def test_band_empty_and_tiny_matrices():
     pl.close()
 
 
-def test_band_no_timeouts():
-    from swift_b200 import _capi as capi
-    import ctypes as C
-    f = C.c_int(-1)
-    capi.check(capi.lib().swift_band_timeout_flag(C.byref(f), 0), "swift_band_timeout_flag")
-    assert f.value == 0
-
-
 @pytest.mark.parametrize("dt", ["float32", "bfloat16", "float16"])
 @pytest.mark.parametrize("N", [128, 136, 200, 256])  # 16-bit rows a multiple of 16 bytes
 @pytest.mark.parametrize("shape", [(1000, 1000, 32), (1500, 1000, 16), (777, 1200, 4), (4096, 4096, 48)])
@@ -295,3 +287,33 @@ def test_band_fp32_accuracy():
     ref = pl.spmm_f64_reference(B.double()).cpu().numpy()
     assert relerr(C.cpu().numpy(), ref) <= 2e-6
     pl.close()
+
+
+@pytest.mark.parametrize("dt", ["bfloat16", "float16"])
+def test_band_16bit_strided_operands(dt):
+    """16-bit B and C as views with leading dimensions beyond N (rows 16-byte multiples, B 16
+    bytes into each row): the TMA boxes follow the strides and the C tile store leaves the
+    columns beyond N untouched."""
+    M, K, rp, ci, val = build("band32_plus_rmat")
+    N = 128
+    tdt = getattr(torch, dt)
+    Bw = torch.from_numpy(gen.dense_uniform(K, N + 16, seed=23)).cuda().to(tdt)
+    B = Bw[:, 8:8 + N]
+    Cw = torch.full((M, N + 24), 7.0, device="cuda", dtype=tdt)
+    C = Cw[:, :N]
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    pl.spmm(B, C_out=C, engine="band")
+    ref = pl.spmm_f64_reference(B.contiguous().double()).cpu().numpy()
+    assert relerr(C.double().cpu().numpy(), ref) <= 1e-2
+    assert torch.all(Cw[:, N:] == 7.0)
+    Cd = pl.spmm(B.contiguous(), engine="band")
+    assert torch.equal(C, Cd)  # the same product as with dense operands
+    pl.close()
+
+
+def test_band_no_timeouts():
+    from swift_b200 import _capi as capi
+    import ctypes as C
+    f = C.c_int(-1)
+    capi.check(capi.lib().swift_band_timeout_flag(C.byref(f), 0), "swift_band_timeout_flag")
+    assert f.value == 0
