@@ -190,22 +190,31 @@ def test_band_autotune_picks_band_and_auto_runs_it():
     pl.close()
 
 
-def test_band_empty_and_tiny_matrices():
-    """No nonzeros at all (every C row written as zeros), and fewer rows than one 64-row group."""
-    B = torch.from_numpy(gen.dense_uniform(300, 128, seed=21)).cuda()
+@pytest.mark.parametrize("dt", ["float32", "bfloat16", "float16"])
+def test_band_empty_and_tiny_matrices(dt):
+    """No nonzeros at all (every C row written as zeros), fewer rows than one 16-row group, and
+    fewer B rows than one 64-row chunk."""
+    tdt = getattr(torch, dt)
+    tol = 1e-5 if dt == "float32" else 1e-2
+    B = torch.from_numpy(gen.dense_uniform(300, 128, seed=21)).cuda().to(tdt)
     rp = np.zeros(501, np.int32)
     pl = Plan.from_csr(rp, np.zeros(0, np.int32), np.zeros(0, np.float32), (500, 300))
-    C = torch.full((500, 128), 5.0, device="cuda")
+    C = torch.full((500, 128), 5.0, device="cuda", dtype=tdt)
     pl.spmm(B, C_out=C, engine="band")
     assert torch.count_nonzero(C).item() == 0
     pl.close()
-    rp, ci = band_pattern(5, 300, 3)
-    val = gen.uniform_values(len(ci), seed=22)
-    pl = Plan.from_csr(rp, ci, val, (5, 300))
-    C = pl.spmm(B, engine="band")
-    ref = oracle.pipeline(5, 300, rp, ci, val, B.cpu().numpy())["C"]
-    assert relerr(C.cpu().numpy(), ref) <= 1e-5
-    pl.close()
+    for M, K in ((5, 300), (300, 40)):
+        rp, ci = band_pattern(M, K, 3)
+        val = gen.uniform_values(len(ci), seed=22)
+        pl = Plan.from_csr(rp, ci, val, (M, K))
+        Bk = B[:K].contiguous()
+        C = pl.spmm(Bk, engine="band")
+        ref = pl.spmm_f64_reference(Bk.double()).cpu().numpy()
+        assert relerr(C.double().cpu().numpy(), ref) <= tol, (M, K)
+        if dt == "float32":
+            ref = oracle.pipeline(M, K, rp, ci, val, Bk.cpu().numpy())["C"]
+            assert relerr(C.cpu().numpy(), ref) <= 1e-5
+        pl.close()
 
 
 @pytest.mark.parametrize("dt", ["float32", "bfloat16", "float16"])

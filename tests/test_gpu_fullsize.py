@@ -10,7 +10,9 @@
   src/Swift_cpu.h:2-78) at N = 32 and 128, normwise max|C - C_ref| / max|C_ref| <= 1e-5 (FP32)
   and <= 1e-12 (FP64), beside the error against the deterministic FP64 GPU product.
 * R-MAT scale 19 (16,777,216 draws) merged with the |i - j| < 32 band: BF16 and FP16 B and C
-  (FP32 accumulation), plain and per-row scaled, within 1e-2 of the FP64 product.
+  (FP32 accumulation), plain and per-row scaled, within 1e-2 of the FP64 product; the band
+  engine (tiles of half-width 31; 16-bit tiles on the tensor cores) in FP32 within 1e-5 and in
+  BF16 / FP16 within 1e-2.
 * The 262,144-node symmetric-normalised R-MAT graph at N = 64: Y = A X, dX = A^T dY and
   dA = SDDMM(dY, X), plain and fused, within 1e-5 of FP64 restatements; FP64 central finite
   differences (directional, torch.autograd.gradcheck fast mode) at 1e-6 on the 4,096-node
@@ -163,6 +165,17 @@ def test_precision_band_16bit_full_size():
         es = trelerr(Cs.double() * cs.double()[:, None], ref)
         print(f"{dt} scaled: vs FP64 {es:.3e}")
         assert es <= 1e-2
+    # the band engine (dense diagonal tiles; 16-bit B on the tensor cores) at full size
+    hist, w = plan.band_profile()
+    assert w == 31  # the |i - j| < 32 band
+    cb = plan.spmm(B32, engine="band")
+    assert trelerr(cb, ref) <= 1e-5
+    for dt in (torch.bfloat16, torch.float16):
+        C = plan.spmm(B32.to(dt), engine="band")
+        e64 = trelerr(C, ref)
+        print(f"{dt} band engine: vs FP64 {e64:.3e}")
+        assert e64 <= 1e-2
+        assert trelerr(C, plan.spmm_f64_reference(B32.to(dt).double())) <= 1e-2
     plan.close()
 
 
