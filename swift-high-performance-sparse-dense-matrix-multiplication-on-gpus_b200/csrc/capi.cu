@@ -27,7 +27,7 @@ size_t plan_device_bytes(const Plan &p) {
                           &p.reside_ptr, &p.reside_row, &p.reside_val, &p.colorblk, &p.blkstart,
                           &p.blkstop, &p.blkptr, &p.rowcopy_b, &p.rowcopy_c, &p.g_row, &p.g_col,
                           &p.g_val, &p.band_tiles, &p.band_ptr, &p.band_idx, &p.band_val, &p.band_dst,
-                          &p.band_mma};
+                          &p.band_mma[0], &p.band_mma[1]};
   size_t s = 0;
   for (const DevBuf *b : bufs) s += b->bytes;
   for (const RowLayout *L : {&p.fwd, &p.bwd, &p.band_rest}) {

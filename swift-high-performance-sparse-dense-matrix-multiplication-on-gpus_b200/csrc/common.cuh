@@ -208,12 +208,13 @@ struct Plan {
   long long band_hist[129] = {};
   bool band_built = false;
   DevBuf band_tiles, band_ptr, band_idx, band_val, band_dst;
-  // the tiles in the tensor-core kernel's A-fragment order (16-bit B): 16-row windows, each row
-  // scaled by a power of two and split into hi + lo parts of B's type, then the rows' inverse
-  // factors; band_mma_dtype is the type they were built for (-1: none; rebuilt on the first
-  // 16-bit product after a build, a refill or a change of type)
-  DevBuf band_mma;
-  int band_mma_dtype = -1;
+  // the tiles in the tensor-core kernel's A-fragment order, one layout per 16-bit type of B
+  // (index 0 BF16, 1 FP16): 16-row windows, each row scaled by a power of two and split into
+  // hi + lo parts of that type, then the rows' inverse factors; built on the first product of
+  // that type after a build or a refill (a buffer per type, so that alternating BF16 and FP16
+  // products rebuild nothing)
+  DevBuf band_mma[2];
+  bool band_mma_built[2] = {false, false};
   RowLayout band_rest;
   std::mutex mu;  // guards lazily built layouts and scratch growth
   // Streams this plan's work was enqueued on, each with an event recorded after its latest

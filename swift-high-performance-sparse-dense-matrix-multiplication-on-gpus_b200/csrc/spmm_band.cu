@@ -712,7 +712,7 @@ static swift_status band_build(Plan &p, int W, cudaStream_t st) {
   const int64_t rows_pad = (int64_t)((p.M + kCtaRows - 1) / kCtaRows) * kCtaRows;
   if (rows_pad * TW >= INT32_MAX) return SWIFT_ERR_OVERFLOW;
   p.band_built = false;
-  p.band_mma_dtype = -1;
+  p.band_mma_built[0] = p.band_mma_built[1] = false;
   SW_TRY(p.band_tiles.alloc(sizeof(float) * (size_t)std::max<int64_t>(rows_pad * TW, 1)));
   SW_CHECK_CUDA(cudaMemsetAsync(p.band_tiles.p, 0, p.band_tiles.bytes, st));
   SW_TRY(p.band_ptr.alloc(sizeof(int) * ((size_t)p.M + 1)));
@@ -752,15 +752,17 @@ static swift_status band_build(Plan &p, int W, cudaStream_t st) {
   return SWIFT_OK;
 }
 
-// The tiles in the tensor-core kernel's fragment order for 16-bit type `dtype` (p.mu held;
-// after band_build).
+// The tiles in the tensor-core kernel's fragment order for 16-bit type `dtype`, in that type's
+// own buffer (p.mu held; after band_build).
 static swift_status band_mma_build(Plan &p, int dtype, cudaStream_t st) {
   const int TW = tile_width(p.band_used_w);
   const int KS = mma_width(TW) / 16;
   const int nblocks = (p.M + kCtaRows - 1) / kCtaRows;
   const int64_t rows = (int64_t)nblocks * kCtaRows;
-  p.band_mma_dtype = -1;
-  SW_TRY(p.band_mma.alloc((size_t)std::max(nblocks, 1) * mma_block_bytes(KS)));
+  const int ti = dtype == SWIFT_BF16 ? 0 : 1;
+  DevBuf &out = p.band_mma[ti];
+  p.band_mma_built[ti] = false;
+  SW_TRY(out.alloc((size_t)std::max(nblocks, 1) * mma_block_bytes(KS)));
   TmpBuf rexp;
   SW_TRY(rexp.alloc(sizeof(int) * (size_t)std::max<int64_t>(rows, 1), st));
   const int rgrid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 255) / 256, (int64_t)p.sm_count * 16));
@@ -770,18 +772,18 @@ static swift_status band_mma_build(Plan &p, int dtype, cudaStream_t st) {
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((threads + 255) / 256, (int64_t)p.sm_count * 16));
   if (dtype == SWIFT_BF16)
     band_mma_fill_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(p.band_tiles.as<float>(), rexp.as<int>(), nblocks, TW, KS,
-                                                              static_cast<unsigned char *>(p.band_mma.p));
+                                                              static_cast<unsigned char *>(out.p));
   else
     band_mma_fill_kernel<__half><<<grid, 256, 0, st>>>(p.band_tiles.as<float>(), rexp.as<int>(), nblocks, TW, KS,
-                                                       static_cast<unsigned char *>(p.band_mma.p));
+                                                       static_cast<unsigned char *>(out.p));
   SW_CHECK_LAUNCH();
-  p.band_mma_dtype = dtype;
+  p.band_mma_built[ti] = true;
   return SWIFT_OK;
 }
 
 swift_status band_refill(Plan &p, cudaStream_t st) {
   if (!p.band_built || p.nnz == 0) return SWIFT_OK;
-  p.band_mma_dtype = -1;  // regrouped on the next 16-bit product
+  p.band_mma_built[0] = p.band_mma_built[1] = false;  // regrouped on the next 16-bit products
   const int grid = (int)std::min<int64_t>(((int64_t)p.nnz + 255) / 256, (int64_t)p.sm_count * 16);
   if (p.val_type == SWIFT_F64)
     band_refill_kernel<double><<<grid, 256, 0, st>>>(p.val.as<double>(), p.nnz, p.band_dst.as<int>(),
@@ -814,7 +816,8 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
     SW_TRY(band_profile(p, st));
     W = p.band_w >= 0 ? p.band_w : kWidths[0];
     if (!p.band_built || p.band_used_w != W) SW_TRY(band_build(p, W, st));
-    if (d.dtype != SWIFT_F32 && p.band_mma_dtype != d.dtype) SW_TRY(band_mma_build(p, d.dtype, st));
+    if (d.dtype != SWIFT_F32 && !p.band_mma_built[d.dtype == SWIFT_BF16 ? 0 : 1])
+      SW_TRY(band_mma_build(p, d.dtype, st));
   }
   if (d.dtype != SWIFT_F32) {
     // 16-bit B and C: the tensor-core kernel, both operands as swizzled 64 x 64 TMA boxes
@@ -823,7 +826,7 @@ swift_status run_band(Plan &p, const DenseArgs &d, const MergeOpts &o, cudaStrea
     SW_TRY(encode_16bit_swizzled(&cmap, d.C, p.M, d.N, d.ldc, d.dtype));
     // the rest first: the row walk writes every C row (zeros where a row has no rest nonzeros)
     SW_TRY(run_merge(p, p.band_rest, d, o, st));
-    const unsigned char *frags = static_cast<const unsigned char *>(p.band_mma.p);
+    const unsigned char *frags = static_cast<const unsigned char *>(p.band_mma[d.dtype == SWIFT_BF16 ? 0 : 1].p);
     if (d.dtype == SWIFT_BF16) return launch_mma_w<__nv_bfloat16>(bmap, cmap, frags, p.M, d.N, W, p.sm_count, st);
     return launch_mma_w<__half>(bmap, cmap, frags, p.M, d.N, W, p.sm_count, st);
   }

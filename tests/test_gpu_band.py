@@ -320,6 +320,24 @@ def test_band_16bit_strided_operands(dt):
     pl.close()
 
 
+
+def test_band_bf16_and_fp16_products_alternate():
+    """BF16 and FP16 products on one plan keep separate tile layouts: alternating them gives the
+    results of the first products bit for bit (and rebuilds nothing)."""
+    M, K, rp, ci, val = build("band32_plus_rmat")
+    B32 = torch.from_numpy(gen.dense_uniform(K, 128, seed=31)).cuda()
+    Bb, Bh = B32.to(torch.bfloat16), B32.half()
+    pl = Plan.from_csr(rp, ci, val, (M, K))
+    Cb = pl.spmm(Bb, engine="band")
+    Ch = pl.spmm(Bh, engine="band")
+    C32 = pl.spmm(B32, engine="band")
+    for _ in range(2):
+        assert torch.equal(pl.spmm(Bb, engine="band"), Cb)
+        assert torch.equal(pl.spmm(Bh, engine="band"), Ch)
+        assert torch.equal(pl.spmm(B32, engine="band"), C32)
+    pl.close()
+
+
 def test_band_no_timeouts():
     from swift_b200 import _capi as capi
     import ctypes as C
