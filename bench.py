@@ -828,6 +828,7 @@ def run_batch(args):
         "config": {"workload": args.workload, "matrices": len(mats), "rows": rows_tot, "nnz": nnz_tot,
                    "N_counts": {str(n): Ns.count(n) for n in (32, 64, 128)}, "task_size": best_U,
                    "task_sizes_by_class": dict(zip(("N<=32", "N<=64", "N>64"), batch.task_sizes())),
+                   "n_split_by_class": dict(zip(("N<=32", "N<=64", "N>64"), batch.n_split())),
                    "autotune_wall_ms": tune_wall_ms, "autotune_best_candidate_ms": tune_ms,
                    "launch": "one persistent kernel per step, replayed as a CUDA graph",
                    "l2": "B and C of the batch (about 5 GB) exceed L2; no flush between steps",

@@ -399,13 +399,22 @@ swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream);
 swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream);
 /* Chooses the merge-path task size (merged positions per sub-warp task) per member class --
  * N <= 32, N <= 64, wider -- by timing whole batch launches: the best of 128, 256, 512 and 1024
- * for every class, then each class on its own against the others' current sizes (operands
- * must be set; each C_i is overwritten with its product).  best_ms = the chosen launch's time,
+ * for every class, then each class on its own against the others' current sizes; then the
+ * N-split of each class (see swift_batch_set_n_split), kept where it is faster (operands must
+ * be set; each C_i is overwritten with its product).  best_ms = the chosen launch's time,
  * best_task_size = the widest class's size. */
 swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, double *best_ms,
                                   int *best_task_size);
 /* The task sizes in use for the three member classes (N <= 32, N <= 64, wider). */
 swift_status swift_batch_get_task_sizes(const swift_batch *batch, int *sizes);
+/* N-split per member class (splits[3], each 1 or 2): with 2, every member of the class whose N
+ * is a multiple of 8 is walked as two column halves, each a separate entry of the launch
+ * (own tasks and split-row scratch) -- half-width B rows per gather, the walk over A twice.
+ * Rebuilds the launch table when operands are set (a graph captured by swift_batch_run_graph
+ * is re-captured on its next call).  SWIFT_ERR_INVALID_ARG for other values. */
+swift_status swift_batch_set_n_split(swift_batch *batch, const int *splits, swift_stream_t stream);
+/* The N-split in use for the three member classes. */
+swift_status swift_batch_get_n_split(const swift_batch *batch, int *splits);
 
 /* ------------------------------------------------------------------ MatrixMarket input */
 /* Reads a MatrixMarket coordinate file into host CSR as the reference's reader does

@@ -23,6 +23,13 @@ struct swift_batch {
   // merge-path task size per member class: N <= 32, N <= 64, wider (each class has its own
   // best grain: narrow rows favour small tasks, wide rows large ones)
   int U[3] = {512, 512, 512};
+  // N-split per member class: 1 walks a member's N columns at once, 2 walks them as two column
+  // halves, each its own table entry (own tasks, split-row scratch and counters), so that each
+  // gathered B row is half as wide and the walk over A runs twice.  Members whose half-width is
+  // not a multiple of 4 columns stay whole.
+  int nsplit[3] = {1, 1, 1};
+  int entries = 0;        // table entries (members, or member halves) of the current table
+  int graph_entries = -1;  // entries the captured graph was made for
   int grid = 0;
   std::vector<swift_plan *> plans;
   // the order the persistent grid walks the members in: flattest column distribution first
@@ -30,6 +37,9 @@ struct swift_batch {
   // distribution gather across their whole B; walking them before the skewed ones measured
   // fastest (batch512: 8.48 ms against 9.7-10.2 ms for shuffled or skewed-first orders).
   std::vector<int> order;
+  // layouts[2i + h]: member i's tasks and scratch for column half h (h = 0 also for a whole
+  // member).  A layout always serves the same member, so its cached tasks stay valid whatever the
+  // N-split (which renumbers the table entries).
   std::vector<std::unique_ptr<swift::RowLayout>> layouts;
   std::vector<unsigned char> h_args;
   std::vector<int> h_shape;
@@ -65,28 +75,41 @@ swift_status on_device(const swift_batch *b) {
   return SWIFT_OK;
 }
 
-// (Re)builds every member's launch record from the stored operands and uploads the table.
+// Column halves member i is walked in under the current N-split (1 or 2).
+int member_split(const swift_batch *b, int i) {
+  const int N = b->ops.N[i], s = b->nsplit[member_class(N)];
+  return (s == 2 && N > 0 && N % 8 == 0) ? 2 : 1;
+}
+
+// (Re)builds every member's launch records from the stored operands and uploads the table:
+// entries in member order, the halves of a split member side by side.
 swift_status build_table(swift_batch *b, cudaStream_t st) {
   const size_t asz = merge_args_size();
   int64_t off = 0;
+  int v = 0;
   for (int k = 0; k < b->count; ++k) {
-    const int i = b->order[k];  // table slot k holds member i
-    b->h_off[k] = off;
-    int64_t items = 0;
-    SW_TRY(merge_batch_member(b->plans[i]->p, *b->layouts[i], b->U[member_class(b->ops.N[i])], b->ops.N[i],
-                              b->ops.B[i], b->ops.ldb[i],
-                              b->ops.C[i], b->ops.ldc[i], b->h_args.data() + asz * k, &b->h_shape[k], &items,
-                              st));
-    off += items;
+    const int i = b->order[k];
+    const int s = member_split(b, i), Nh = b->ops.N[i] / s;
+    for (int h = 0; h < s; ++h, ++v) {
+      std::unique_ptr<RowLayout> &L = b->layouts[2 * (size_t)i + h];
+      if (!L) L.reset(new RowLayout());
+      b->h_off[v] = off;
+      int64_t items = 0;
+      const void *B = b->ops.B[i] ? static_cast<const float *>(b->ops.B[i]) + (size_t)h * Nh : nullptr;
+      void *C = b->ops.C[i] ? static_cast<float *>(b->ops.C[i]) + (size_t)h * Nh : nullptr;
+      SW_TRY(merge_batch_member(b->plans[i]->p, *L, b->U[member_class(b->ops.N[i])], Nh, B,
+                                b->ops.ldb[i], C, b->ops.ldc[i], b->h_args.data() + asz * v, &b->h_shape[v],
+                                &items, st));
+      off += items;
+    }
   }
-  b->h_off[b->count] = off;
-  if (b->count > 0) {
-    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_args.p, b->h_args.data(), asz * b->count, cudaMemcpyHostToDevice, st));
-    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_shape.p, b->h_shape.data(), sizeof(int) * b->count,
-                                  cudaMemcpyHostToDevice, st));
+  b->entries = v;
+  b->h_off[v] = off;
+  if (v > 0) {
+    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_args.p, b->h_args.data(), asz * v, cudaMemcpyHostToDevice, st));
+    SW_CHECK_CUDA(cudaMemcpyAsync(b->d_shape.p, b->h_shape.data(), sizeof(int) * v, cudaMemcpyHostToDevice, st));
   }
-  SW_CHECK_CUDA(cudaMemcpyAsync(b->d_off.p, b->h_off.data(), sizeof(int64_t) * (b->count + 1),
-                                cudaMemcpyHostToDevice, st));
+  SW_CHECK_CUDA(cudaMemcpyAsync(b->d_off.p, b->h_off.data(), sizeof(int64_t) * (v + 1), cudaMemcpyHostToDevice, st));
   SW_CHECK_CUDA(cudaStreamSynchronize(st));  // the host table may change after return
   b->ready = true;
   return SWIFT_OK;
@@ -94,7 +117,7 @@ swift_status build_table(swift_batch *b, cudaStream_t st) {
 
 swift_status launch(swift_batch *b, cudaStream_t st) {
   return launch_merge_batch(b->d_args.p, b->d_shape.as<int>(), static_cast<const int64_t *>(b->d_off.p),
-                            b->count, b->grid, st);
+                            b->entries, b->grid, st);
 }
 
 swift_status check_ready(const swift_batch *b, const char *where) {
@@ -151,10 +174,11 @@ swift_status swift_batch_create(swift_plan *const *plans, int count, swift_strea
     for (int i = 0; i < count; ++i) b->order[(size_t)i] = i;
     std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return skew[(size_t)x] < skew[(size_t)y]; });
   }
-  for (int i = 0; i < count; ++i) b->layouts.emplace_back(new RowLayout());
-  b->h_args.assign(merge_args_size() * (size_t)std::max(count, 1), 0);
-  b->h_shape.assign((size_t)std::max(count, 1), 0);
-  b->h_off.assign((size_t)count + 1, 0);
+  const size_t cap = 2 * (size_t)std::max(count, 1);  // table entries: every member split in two at most
+  b->layouts.resize(cap);
+  b->h_args.assign(merge_args_size() * cap, 0);
+  b->h_shape.assign(cap, 0);
+  b->h_off.assign(cap + 1, 0);
   SW_TRY(b->d_args.alloc(b->h_args.size()));
   SW_TRY(b->d_shape.alloc(sizeof(int) * b->h_shape.size()));
   SW_TRY(b->d_off.alloc(sizeof(int64_t) * b->h_off.size()));
@@ -198,6 +222,12 @@ swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream) {
 
 swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream) {
   SW_TRY(check_ready(batch, "swift_batch_run_graph"));
+  if (batch->exec && batch->graph_entries != batch->entries) {  // the table's entry count changed
+    cudaGraphExecDestroy(batch->exec);
+    cudaGraphDestroy(batch->graph);
+    batch->exec = nullptr;
+    batch->graph = nullptr;
+  }
   if (!batch->exec) {
     // captured on a private stream (the legacy default stream cannot be captured)
     if (!batch->cap) SW_CHECK_CUDA(cudaStreamCreateWithFlags(&batch->cap, cudaStreamNonBlocking));
@@ -212,6 +242,7 @@ swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream) {
     SW_CHECK_CUDA(ce);
     batch->graph = g;
     SW_CHECK_CUDA(cudaGraphInstantiate(&batch->exec, batch->graph, 0));
+    batch->graph_entries = batch->entries;
   }
   SW_CHECK_CUDA(cudaGraphLaunch(batch->exec, to_stream(stream)));
   return SWIFT_OK;
@@ -224,7 +255,7 @@ swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, dou
   cudaEvent_t e0, e1;
   SW_CHECK_CUDA(cudaEventCreate(&e0));
   SW_CHECK_CUDA(cudaEventCreate(&e1));
-  // ms per launch with the task sizes in `U`, or < 0 on failure
+  // ms per launch with the task sizes in `U` (and the current N-split), or < 0 on failure
   auto time_sizes = [&](const int (&U)[3], swift_status &rc) -> double {
     for (int c = 0; c < 3; ++c) batch->U[c] = U[c];
     rc = build_table(batch, st);
@@ -265,6 +296,19 @@ swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, dou
       if (ms < best) { best = ms; bestU[c] = u; }
     }
   }
+  // then the N-split of each class present with members that can be halved
+  bool splittable[3] = {false, false, false};
+  for (int i = 0; i < batch->count; ++i)
+    if (batch->ops.N[i] > 0 && batch->ops.N[i] % 8 == 0) splittable[member_class(batch->ops.N[i])] = true;
+  for (int c = 0; c < 3 && rc == SWIFT_OK; ++c) {
+    if (!splittable[c]) continue;
+    const int keep = batch->nsplit[c];
+    batch->nsplit[c] = keep == 1 ? 2 : 1;
+    const double ms = time_sizes(bestU, rc);
+    if (rc != SWIFT_OK) break;
+    if (ms < best) best = ms;
+    else batch->nsplit[c] = keep;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   for (int c = 0; c < 3; ++c) batch->U[c] = bestU[c];
@@ -278,6 +322,21 @@ swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, dou
 swift_status swift_batch_get_task_sizes(const swift_batch *batch, int *sizes) {
   if (!batch || !sizes) return SWIFT_ERR_INVALID_ARG;
   for (int c = 0; c < 3; ++c) sizes[c] = batch->U[c];
+  return SWIFT_OK;
+}
+
+swift_status swift_batch_set_n_split(swift_batch *batch, const int *splits, swift_stream_t stream) {
+  if (!batch || !splits) return SWIFT_ERR_INVALID_ARG;
+  for (int c = 0; c < 3; ++c)
+    if (splits[c] != 1 && splits[c] != 2) return SWIFT_ERR_INVALID_ARG;
+  SW_TRY(on_device(batch));
+  for (int c = 0; c < 3; ++c) batch->nsplit[c] = splits[c];
+  return batch->ready ? build_table(batch, to_stream(stream)) : SWIFT_OK;
+}
+
+swift_status swift_batch_get_n_split(const swift_batch *batch, int *splits) {
+  if (!batch || !splits) return SWIFT_ERR_INVALID_ARG;
+  for (int c = 0; c < 3; ++c) splits[c] = batch->nsplit[c];
   return SWIFT_OK;
 }
 

@@ -154,6 +154,8 @@ _SIGS = [
     ("swift_batch_run_graph", C.c_int, [_P, _P]),
     ("swift_batch_autotune", C.c_int, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     ("swift_batch_get_task_sizes", C.c_int, [_P, _P]),
+    ("swift_batch_set_n_split", C.c_int, [_P, _P, _P]),
+    ("swift_batch_get_n_split", C.c_int, [_P, _P]),
     ("swift_mtx_read", C.c_int, [C.c_char_p, C.c_int] + [C.POINTER(C.c_int)] * 4
      + [C.POINTER(C.POINTER(C.c_int))] * 2 + [C.POINTER(C.c_void_p), C.POINTER(C.c_int)]),
     ("swift_host_free", None, [_P]),

@@ -425,8 +425,8 @@ class Batch:
         capi.check(capi.lib().swift_batch_run_graph(self._h, _stream_ptr(stream)), "swift_batch_run_graph")
 
     def autotune(self, stream=None):
-        """Chooses the task size per member class (N <= 32, N <= 64, wider); returns (the widest
-        class's task size, ms per run)."""
+        """Chooses the task size and the N-split per member class (N <= 32, N <= 64, wider);
+        returns (the widest class's task size, ms per run)."""
         ms, U = C.c_double(0), C.c_int(0)
         capi.check(capi.lib().swift_batch_autotune(self._h, _stream_ptr(stream), C.byref(ms), C.byref(U)),
                    "swift_batch_autotune")
@@ -437,6 +437,19 @@ class Batch:
         out = (C.c_int * 3)()
         capi.check(capi.lib().swift_batch_get_task_sizes(self._h, out), "swift_batch_get_task_sizes")
         return list(out)
+
+    def n_split(self):
+        """The N-split (1 or 2 column halves) in use for the member classes N <= 32, N <= 64 and
+        wider."""
+        out = (C.c_int * 3)()
+        capi.check(capi.lib().swift_batch_get_n_split(self._h, out), "swift_batch_get_n_split")
+        return list(out)
+
+    def set_n_split(self, splits, stream=None):
+        """Walk the members of each class in 1 or 2 column halves (members whose N is a multiple
+        of 8); rebuilds the launch table when operands are set."""
+        arr = (C.c_int * 3)(*[int(x) for x in splits])
+        capi.check(capi.lib().swift_batch_set_n_split(self._h, arr, _stream_ptr(stream)), "swift_batch_set_n_split")
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

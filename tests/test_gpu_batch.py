@@ -1,6 +1,7 @@
 """Batched products in one persistent launch (swift_batch_*): every member against the
 deterministic FP64 product of its own plan (normwise 1e-5), bit-identical repeats, CUDA-graph
-replay equal to the plain launch, new operands picked up by a captured graph, autotuning."""
+replay equal to the plain launch, new operands picked up by a captured graph, autotuning,
+the N-split (members walked as two column halves) bit-equal to the unsplit launch."""
 import numpy as np
 import pytest
 
@@ -85,12 +86,51 @@ def test_batch_autotune_keeps_results():
     sizes = b.task_sizes()
     assert U in (128, 256, 512, 1024) and ms_run > 0
     assert sizes[2] == U and all(s in (128, 256, 512, 1024) for s in sizes)
+    assert all(s in (1, 2) for s in b.n_split())
     for c in Cs:
         c.fill_(float("nan"))
     b.run()
     torch.cuda.synchronize()
     for p, B, C in zip(plans, Bs, Cs):
         assert relerr(C, p.spmm_f64_reference(B.double())) <= 1e-5
+    b.close()
+
+
+@pytest.mark.parametrize("splits", [(2, 2, 2), (1, 2, 1), (2, 1, 2)])
+def test_batch_n_split_matches_unsplit(splits):
+    """Members walked as two column halves (each its own launch entry, tasks and split-row
+    scratch): every member within 1e-5 of its FP64 product and bit-equal to the unsplit batch
+    (each C element is summed in the same order); members whose N is not a multiple of 8 stay
+    whole; a captured graph is re-captured when the entry count changes."""
+    ms = members(24, seed=6)
+    plans, Bs, Cs = build(ms, 3)
+    b = Batch(plans)
+    b.set_operands(Bs, Cs)
+    b.run_graph()
+    torch.cuda.synchronize()
+    whole = [c.clone() for c in Cs]
+    b.set_n_split(splits)
+    assert b.n_split() == list(splits)
+    for c in Cs:
+        c.fill_(float("nan"))
+    b.run()
+    torch.cuda.synchronize()
+    for p, B, C, W, m in zip(plans, Bs, Cs, whole, ms):
+        assert relerr(C, p.spmm_f64_reference(B.double())) <= 1e-5, m["kind"]
+        assert torch.equal(C, W), m["kind"]
+    for c in Cs:
+        c.fill_(float("nan"))
+    b.run_graph()  # the table now has more entries: the graph is captured again
+    torch.cuda.synchronize()
+    for C, W in zip(Cs, whole):
+        assert torch.equal(C, W)
+    b.set_n_split((1, 1, 1))
+    b.run_graph()
+    torch.cuda.synchronize()
+    for C, W in zip(Cs, whole):
+        assert torch.equal(C, W)
+    with pytest.raises(capi.SwiftError):
+        b.set_n_split((3, 1, 1))
     b.close()
 
 
