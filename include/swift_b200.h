@@ -195,6 +195,9 @@ swift_status swift_device_check(int *sm_count, int *cc_major, int *cc_minor);
  * device.  Synchronises `stream` once (sizes of the format are read back). */
 swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
                                swift_stream_t stream, swift_plan **out);
+/* Releases the plan's device memory once the work it enqueued on each stream it ran on is done
+ * (stream-ordered: the host does not wait and other streams are not stalled; when the plan was
+ * used inside a stream capture, after a device synchronisation). */
 swift_status swift_plan_destroy(swift_plan *plan);
 swift_status swift_plan_get_stats(const swift_plan *plan, swift_plan_stats *out);
 /* New values for the plan's fixed pattern (nnz values of the plan's value type, CSR order,
@@ -382,7 +385,9 @@ swift_status swift_plan_get_rowwise_params(swift_plan *plan, int N, swift_dtype 
 typedef struct swift_batch swift_batch;
 swift_status swift_batch_create(swift_plan *const *plans, int count, swift_stream_t stream,
                                 swift_batch **out);
-/* Synchronises the device before freeing the members' buffers. */
+/* Releases the batch's device memory once its own launches are done (stream-ordered, as
+ * swift_plan_destroy; after a device synchronisation when a launch was captured into a
+ * caller's graph). */
 swift_status swift_batch_destroy(swift_batch *batch);
 /* Ns[i], B[i], ldb[i], C[i], ldc[i] per member (device pointers, row-major).  N_i <= 128 with
  * 16-byte aligned operands (N_i % 4 == 0), or N_i <= 32 otherwise.  Builds the members' task

@@ -124,13 +124,33 @@ void note_use(Plan &p, cudaStream_t st) {
 
 UseNote::~UseNote() { note_use(p, st); }
 
+cudaStream_t alloc_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[128] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
+    streams[dev] = nullptr;
+  return streams[dev];
+}
+
+cudaStream_t &release_stream() {
+  thread_local cudaStream_t s = nullptr;
+  return s;
+}
+
+cudaStream_t release_stream_after(const std::vector<std::pair<cudaStream_t, cudaEvent_t>> &uses,
+                                  bool sync_device) {
+  if (sync_device) cudaDeviceSynchronize();
+  cudaStream_t fs = nullptr;
+  if (cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  for (auto &u : uses) cudaStreamWaitEvent(fs, u.second, 0);
+  return fs;
+}
+
 Plan::~Plan() {
-  // the device buffers are freed after this body: wait for the work that reads them
-  if (sync_device_on_destroy) {
-    cudaDeviceSynchronize();
-  } else {
-    for (auto &u : uses) cudaEventSynchronize(u.second);
-  }
+  // swift_plan_destroy has ordered the buffers' release after the plan's own work
   for (auto &u : uses) cudaEventDestroy(u.second);
 }
 }  // namespace swift
@@ -230,7 +250,19 @@ swift_status swift_plan_create(const swift_csr *A, const swift_plan_opts *opts,
 
 swift_status swift_plan_destroy(swift_plan *plan) {
   if (!plan) return SWIFT_ERR_INVALID_ARG;
-  delete plan;  // ~Plan waits for the plan's own streams (every stream if graphs hold it)
+  Plan &p = plan->p;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != p.device) cudaSetDevice(p.device);
+  cudaStream_t fs;
+  {
+    std::lock_guard<std::mutex> g(p.use_mu);
+    fs = release_stream_after(p.uses, p.sync_device_on_destroy);
+  }
+  if (prev >= 0 && prev != p.device) cudaSetDevice(prev);
+  // the buffers go back to the pool once the plan's own streams reach this point (every stream
+  // when a captured graph holds the plan); the host does not wait
+  delete_releasing(plan, p.device, fs);
   return SWIFT_OK;
 }
 

@@ -42,6 +42,34 @@ void set_last_error(const char *where, const char *what);
 inline cudaStream_t S(swift_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---------------------------------------------------------------- device buffers
+// Device allocations come from the device's default memory pool, on a private per-device
+// stream (alloc_stream) that is synchronised before the buffer is handed out, so a buffer is
+// ready for any stream.  A buffer is returned to the pool either stream-ordered on
+// release_stream() -- set by swift_plan_destroy / swift_batch_destroy while they delete a plan
+// or batch, to a stream that waits for that object's own work, so destruction neither blocks
+// the host nor stalls other streams -- or, when a buffer is replaced or freed elsewhere, after a
+// device-wide synchronisation (the ordering a plain cudaFree gives).
+cudaStream_t alloc_stream();
+cudaStream_t &release_stream();  // thread-local; null outside the destroy paths
+// A private stream (of the current device) that waits for the work recorded in `uses` -- after
+// a device-wide synchronisation when that record is incomplete -- for a destroy path to release
+// buffers on; null when no stream can be made (buffers are then freed after a device
+// synchronisation).
+cudaStream_t release_stream_after(const std::vector<std::pair<cudaStream_t, cudaEvent_t>> &uses,
+                                  bool sync_device);
+// Deletes a plan or batch on its own device with its buffers released on `fs`.
+template <class Obj>
+void delete_releasing(Obj *o, int device, cudaStream_t fs) {
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != device) cudaSetDevice(device);
+  release_stream() = fs;
+  delete o;
+  release_stream() = nullptr;
+  if (fs) cudaStreamDestroy(fs);  // its frees still run, after the waited-for work
+  if (prev >= 0 && prev != device) cudaSetDevice(prev);
+}
+
 // Owning device allocation (plan lifetime).  Size in bytes; never shared.
 struct DevBuf {
   void *p = nullptr;
@@ -56,17 +84,27 @@ struct DevBuf {
   }
   ~DevBuf() { reset(); }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (cudaStream_t rs = release_stream()) {
+        cudaFreeAsync(p, rs);
+      } else {
+        cudaDeviceSynchronize();
+        cudaFreeAsync(p, alloc_stream());
+      }
+    }
     p = nullptr;
     bytes = 0;
   }
   swift_status alloc(size_t n) {
     reset();
     if (n == 0) n = 16;  // keep every pointer valid and 16-byte aligned
-    cudaError_t e = cudaMalloc(&p, n);
+    cudaStream_t s = alloc_stream();
+    cudaError_t e = s ? cudaMallocAsync(&p, n, s) : cudaErrorInvalidResourceHandle;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
+      if (p) cudaFreeAsync(p, s);
       p = nullptr;
-      set_last_error("cudaMalloc", cudaGetErrorString(e));
+      set_last_error("cudaMallocAsync", cudaGetErrorString(e));
       return SWIFT_ERR_ALLOC;
     }
     bytes = n;

@@ -50,7 +50,16 @@ struct swift_batch {
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // Streams the batch launched on, each with an event recorded after its latest launch, so that
+  // destroying the batch waits for its own launches only.  A launch made while the caller's
+  // stream is being captured (or beyond kMaxUses streams) can run later on any stream: then
+  // destruction waits for the whole device.
+  static constexpr int kMaxUses = 16;
+  std::vector<std::pair<cudaStream_t, cudaEvent_t>> uses;
+  bool sync_device_on_destroy = false;
   ~swift_batch() {
+    // swift_batch_destroy has ordered the buffers' release after the batch's own launches
+    for (auto &u : uses) cudaEventDestroy(u.second);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (cap) cudaStreamDestroy(cap);
@@ -118,6 +127,28 @@ swift_status build_table(swift_batch *b, cudaStream_t st) {
 swift_status launch(swift_batch *b, cudaStream_t st) {
   return launch_merge_batch(b->d_args.p, b->d_shape.as<int>(), static_cast<const int64_t *>(b->d_off.p),
                             b->entries, b->grid, st);
+}
+
+// Records that the batch's work was enqueued on `st` (after the enqueue).
+void note_use(swift_batch *b, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    b->sync_device_on_destroy = true;
+    return;
+  }
+  for (auto &u : b->uses)
+    if (u.first == st) {
+      cudaEventRecord(u.second, st);
+      return;
+    }
+  cudaEvent_t ev = nullptr;
+  if ((int)b->uses.size() >= swift_batch::kMaxUses ||
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+    b->sync_device_on_destroy = true;
+    return;
+  }
+  cudaEventRecord(ev, st);
+  b->uses.emplace_back(st, ev);
 }
 
 swift_status check_ready(const swift_batch *b, const char *where) {
@@ -189,8 +220,14 @@ swift_status swift_batch_create(swift_plan *const *plans, int count, swift_strea
 
 swift_status swift_batch_destroy(swift_batch *batch) {
   if (!batch) return SWIFT_ERR_INVALID_ARG;
-  cudaDeviceSynchronize();  // members' buffers may still be in use by a launch in flight
-  delete batch;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != batch->device) cudaSetDevice(batch->device);
+  cudaStream_t fs = release_stream_after(batch->uses, batch->sync_device_on_destroy);
+  if (prev >= 0 && prev != batch->device) cudaSetDevice(prev);
+  // the members' layouts go back to the pool once the batch's own launches are done; the host
+  // does not wait
+  delete_releasing(batch, batch->device, fs);
   return SWIFT_OK;
 }
 
@@ -217,7 +254,9 @@ swift_status swift_batch_set_operands(swift_batch *batch, const int *Ns, const v
 
 swift_status swift_batch_run(swift_batch *batch, swift_stream_t stream) {
   SW_TRY(check_ready(batch, "swift_batch_run"));
-  return launch(batch, to_stream(stream));
+  const swift_status rc = launch(batch, to_stream(stream));
+  note_use(batch, to_stream(stream));
+  return rc;
 }
 
 swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream) {
@@ -244,7 +283,9 @@ swift_status swift_batch_run_graph(swift_batch *batch, swift_stream_t stream) {
     SW_CHECK_CUDA(cudaGraphInstantiate(&batch->exec, batch->graph, 0));
     batch->graph_entries = batch->entries;
   }
-  SW_CHECK_CUDA(cudaGraphLaunch(batch->exec, to_stream(stream)));
+  const cudaError_t le = cudaGraphLaunch(batch->exec, to_stream(stream));
+  note_use(batch, to_stream(stream));
+  SW_CHECK_CUDA(le);
   return SWIFT_OK;
 }
 
@@ -252,6 +293,11 @@ swift_status swift_batch_autotune(swift_batch *batch, swift_stream_t stream, dou
                                   int *best_task_size) {
   SW_TRY(check_ready(batch, "swift_batch_autotune"));
   cudaStream_t st = to_stream(stream);
+  struct Noted {  // every exit path records the autotune launches
+    swift_batch *b;
+    cudaStream_t s;
+    ~Noted() { note_use(b, s); }
+  } noted{batch, st};
   cudaEvent_t e0, e1;
   SW_CHECK_CUDA(cudaEventCreate(&e0));
   SW_CHECK_CUDA(cudaEventCreate(&e1));

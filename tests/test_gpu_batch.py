@@ -134,6 +134,37 @@ def test_batch_n_split_matches_unsplit(splits):
     b.close()
 
 
+def test_destroy_waits_for_its_own_streams_only():
+    """Destroying a batch or a plan waits for the launches it enqueued, not for the device: with
+    another stream busy (a bounded spin of about a second), both destroys return while that
+    stream is still running, and the products they waited for are complete and correct."""
+    ms = members(6, seed=11, extra=False)
+    plans, Bs, Cs = build(ms, 4)
+    b = Batch(plans)
+    b.set_operands(Bs, Cs)
+    work, busy = torch.cuda.Stream(), torch.cuda.Stream()
+    b.run(stream=work)
+    torch.cuda.synchronize()
+    p0, B0 = plans[0], Bs[0]
+    C0 = torch.empty_like(Cs[0])
+    with torch.cuda.stream(busy):
+        torch.cuda._sleep(int(2e9))  # about a second of SM clock on this stream only
+    for c in Cs:
+        c.fill_(float("nan"))
+    b.run(stream=work)
+    p0.spmm(B0, C_out=C0, stream=work)
+    b.close()
+    p0.close()
+    assert not busy.query()  # neither destroy waited for the busy stream
+    work.synchronize()
+    for p, B, C in zip(plans[1:], Bs[1:], Cs[1:]):
+        assert relerr(C, p.spmm_f64_reference(B.double())) <= 1e-5
+    assert torch.isfinite(C0).all() and torch.isfinite(Cs[0]).all()
+    torch.cuda.synchronize()
+    for p in plans[1:]:
+        p.close()
+
+
 def test_batch_rejects_unsupported():
     m = members(2, seed=2, extra=False)
     plans, Bs, Cs = build(m, 2)
