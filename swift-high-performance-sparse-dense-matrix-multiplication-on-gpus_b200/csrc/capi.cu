@@ -124,15 +124,28 @@ void note_use(Plan &p, cudaStream_t st) {
 
 UseNote::~UseNote() { note_use(p, st); }
 
+// The current device's allocation stream, made once per device and CUDA context: after a
+// cudaDeviceReset the old stream died with its context, and a new one is made in the new one.
 cudaStream_t alloc_stream() {
   static std::mutex mu;
-  static cudaStream_t streams[128] = {};
+  struct Entry {
+    unsigned long long ctx = 0;
+    cudaStream_t s = nullptr;
+  };
+  static Entry streams[128];
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  if (cudaSetDevice(dev) != cudaSuccess) return nullptr;  // the device's primary context current
+  unsigned long long id = 0;
+  if (current_context_id(&id) != SWIFT_OK) return nullptr;
   std::lock_guard<std::mutex> g(mu);
-  if (!streams[dev] && cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking) != cudaSuccess)
-    streams[dev] = nullptr;
-  return streams[dev];
+  Entry &e = streams[dev];
+  if (!e.s || e.ctx != id) {
+    e.s = nullptr;
+    if (cudaStreamCreateWithFlags(&e.s, cudaStreamNonBlocking) != cudaSuccess) e.s = nullptr;
+    e.ctx = id;
+  }
+  return e.s;
 }
 
 cudaStream_t &release_stream() {

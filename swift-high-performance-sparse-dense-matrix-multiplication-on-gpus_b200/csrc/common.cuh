@@ -49,6 +49,9 @@ inline cudaStream_t S(swift_stream_t s) { return reinterpret_cast<cudaStream_t>(
 // or batch, to a stream that waits for that object's own work, so destruction neither blocks
 // the host nor stalls other streams -- or, when a buffer is replaced or freed elsewhere, after a
 // device-wide synchronisation (the ordering a plain cudaFree gives).
+// Id of the CUDA context current on this thread (cuCtxGetId through the runtime's driver entry
+// points): tells a reset device's new context from the destroyed one.
+swift_status current_context_id(unsigned long long *id);
 cudaStream_t alloc_stream();
 cudaStream_t &release_stream();  // thread-local; null outside the destroy paths
 // A private stream (of the current device) that waits for the work recorded in `uses` -- after

@@ -33,6 +33,8 @@ struct ScratchAddr {
 };
 ScratchAddr g_addr[kMaxDevices];
 
+}  // namespace
+
 // cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (no libcuda link).
 typedef CUresult (*ctx_get_current_fn)(CUcontext *);
 typedef CUresult (*ctx_get_id_fn)(CUcontext, unsigned long long *);
@@ -59,6 +61,8 @@ swift_status current_context_id(unsigned long long *id) {
   }
   return SWIFT_OK;
 }
+
+namespace {
 
 // Device address of the array on the current device, looked up once per device and context
 // (host code cannot use the symbol itself: on the host it names a host-side stand-in).
