@@ -740,6 +740,7 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
   const int p = (int)(d0 - hdr.x);
   const int pn = (int)((d0 + a.U < a.total ? d0 + a.U : a.total) - hdr.y);
   const bool inb = lsl * VB < a.N;
+  const bool full_lanes = a.N == H * VB;  // every lane of the sub-warp in range (warp-uniform)
   // dY rows are consumed in row order.  For SDDMM alone (registers to spare) the next row's
   // vector is fetched when the walk enters a row, so its latency overlaps the current row's
   // gathers; the fused passes load it on entry.
@@ -824,6 +825,41 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
       stage[j] = e;
     }
     __syncwarp(sgmask);
+    if (!PREU && m == 32 && full_lanes) {
+      // a full chunk with every lane in range: unconditional loads, no per-slot checks
+#pragma unroll 1
+      for (int k = 0; k < 32; k += UNR) {
+        T part[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)(uint32_t)stage[k + u].x * g_ld));
+        const bool starts = (rs >> k) & 0xFu;
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          if (starts) {
+            while (q0 + k + u == pe) finish_and_advance();
+          }
+          if (DOY || DODX) {
+            const T w = F64 ? vstage[k + u] : (T)__int_as_float(stage[k + u].y);
+            x[u].template fma_into<true>(acc, w);
+          }
+          if (DODA) {
+            T d = T(0);
+#pragma unroll
+            for (int e = 0; e < VB; ++e) d = fma(urow[e], x[u].v[e], d);
+            part[u] = d;
+          }
+        }
+        if (DODA) {
+          constexpr bool HALF = DODX && H >= 4;
+          constexpr int RW = HALF ? H : SG;
+          const int rl = HALF ? lsl : sl;
+          const T r = reduce4<T, RW>(part[0], part[1], part[2], part[3], rl, sgmask);
+          const int idx = ((rl & (RW / 2)) ? 2 : 0) + ((rl & (RW / 4)) ? 1 : 0);
+          if ((!HALF || role == 0) && (rl & (RW / 4 - 1)) == 0) dA[q0 + k + idx] = r;
+        }
+      }
+      continue;
+    }
     for (int k = 0; k < m; k += UNR) {
       T part[UNR];
 #pragma unroll
