@@ -832,12 +832,7 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
         T part[UNR];
 #pragma unroll
         for (int u = 0; u < UNR; ++u) x[u].load(reinterpret_cast<const T *>(Gl + (uint64_t)(uint32_t)stage[k + u].x * g_ld));
-        const bool starts = (rs >> k) & 0xFu;
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-          if (starts) {
-            while (q0 + k + u == pe) finish_and_advance();
-          }
+        auto slot = [&](int u) {
           if (DOY || DODX) {
             const T w = F64 ? vstage[k + u] : (T)__int_as_float(stage[k + u].y);
             x[u].template fma_into<true>(acc, w);
@@ -848,6 +843,16 @@ __global__ void __launch_bounds__(256, MINB) merge_bwd_kernel(const BwdArgs ba) 
             for (int e = 0; e < VB; ++e) d = fma(urow[e], x[u].v[e], d);
             part[u] = d;
           }
+        };
+        if ((rs >> k) & 0xFu) {  // a row starts in this group: look for row ends slot by slot
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) {
+            while (q0 + k + u == pe) finish_and_advance();
+            slot(u);
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) slot(u);
         }
         if (DODA) {
           constexpr bool HALF = DODX && H >= 4;
