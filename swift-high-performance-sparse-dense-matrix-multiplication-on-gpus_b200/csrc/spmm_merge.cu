@@ -1349,11 +1349,13 @@ swift_status run_merge(Plan &p, RowLayout &L, const DenseArgs &d, const MergeOpt
 
 namespace {
 
-constexpr int bwd_minb(int VB, int AB, bool DODX) {
-  // FP32 [Y | dX] pass with 16-byte vectors: five blocks per SM (48 registers, 16 bytes of
-  // spill) hide more gather latency than the estimate's four (measured on the 262,144-node
-  // graph at N = 64: 0.447 ms against 0.467 at four blocks and 0.686 at six, 160 bytes spilled)
-  if (VB == 4 && AB == 4 && DODX) return 5;
+constexpr int bwd_minb(int VB, int AB, int SG, bool DOY, bool DODX) {
+  // The FP32 fused passes with 16-byte vectors at N = 64 -- [Y | dX] in 32-lane sub-warps and
+  // Y + dA in 16-lane ones -- run five blocks per SM (48 registers, 16-44 bytes of spill): that
+  // hides more gather latency than the estimate's four.  Measured on the 262,144-node graph:
+  // [Y | dX] 0.447 ms against 0.467 at four blocks and 0.686 at six (160 bytes spilled); Y + dA
+  // 0.573 against 0.585 ms.
+  if (VB == 4 && AB == 4 && DOY && ((DODX && SG == 32) || (!DODX && SG == 16))) return 5;
   const int regs = 32 + (VB * AB / 4) * 6 + 4 * AB / 4 + (DODX ? 4 : 0);
   const int b = 65536 / (256 * regs);
   return b < 1 ? 1 : (b > 8 ? 8 : b);
@@ -1364,7 +1366,7 @@ swift_status launch_bwd(const BwdArgs &ba, cudaStream_t st) {
   constexpr int G = 32 / SG;
   const int64_t warps = ((int64_t)ba.m.ntasks + G - 1) / G;
   if (warps == 0) return SWIFT_OK;
-  merge_bwd_kernel<T, VB, SG, DOY, DODA, DODX, bwd_minb(VB, (int)sizeof(T), DODX)>
+  merge_bwd_kernel<T, VB, SG, DOY, DODA, DODX, bwd_minb(VB, (int)sizeof(T), SG, DOY, DODX)>
       <<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(ba);
   SW_CHECK_LAUNCH();
   return SWIFT_OK;
